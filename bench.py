@@ -1,0 +1,388 @@
+"""Benchmark of the B200 vertical advance (column-steps/s).
+
+Workload (N=1): a whole 1 deg x 1 deg globe, 180 x 360 = 64,800 columns,
+nAlts = 50, 6 neutral species, FP64, dt = 2 s: the batched, graph-captured
+forward of the 1-degree configuration.  A "step" is one RK4 vertical step
+(producers, gather, 4 stages, 5 boundary passes, scatter) of every column.
+Inputs are seeded synthetic columns (gitm_b200/synthetic.py); the state
+(about 0.9 GB) is larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank advances its own globe (an ensemble member
+seeded by rank): weak scaling, no data exchange in the timed loop.
+`--impl reference` times the CPU restatement of the reference (the oracle)
+on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "column-steps/s, 1 deg grid (64,800 columns x 50 alts, FP64 RK4 vertical step)"
+UNIT = "column-steps/s"
+DT = 2.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--deg", type=float, default=1.0, help="grid spacing in degrees")
+    ap.add_argument("--n-alts", type=int, default=50)
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--plain-steps", type=int, default=30)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def opcount(n_alts: int) -> float:
+    with open(os.path.join(ROOT, "tests", "golden", "opcount.json")) as f:
+        d = json.load(f)
+    return float(d["rusanov"][str(n_alts)]["flop_eq_per_column_step"])
+
+
+def profile_traffic():
+    """DRAM bytes per column-step of the step kernel from the committed ncu
+    summary (profiles/vert_step_kernel_globe1deg.md), or None."""
+    p = os.path.join(ROOT, "profiles", "vert_step_kernel_globe1deg.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_column_step:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def algorithmic_bytes_per_column_step(n_alts: int) -> float:
+    """Compulsory HBM bytes of one launch per column (state read once, written
+    once): reads NDensityS(6), IDensityS advected(2) + passive boundary cells,
+    Rho, Temperature, Velocity(3), VerticalVelocity(6), IVelocity up, eddy;
+    writes the same state, electrons, LogNS(6), NDensity."""
+    G = n_alts + 4
+    reads = (6 + 2 + 1 + 1 + 3 + 6 + 1 + 1) * G + 7 * G  # passive ions read for the e- sum
+    writes = (6 + 2 + 1 + 1 + 1 + 3 + 6 + 6 + 1) * G + 7 * 11
+    return 8.0 * (reads + writes)
+
+
+def measure_fp64_peak(torch, device) -> float:
+    """Dense FP64 GEMM throughput (cuBLAS DGEMM through torch), TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_baseline(m, seconds: float, threads: int | None = None) -> dict:
+    """The oracle (CPU restatement of the reference) on the host cores on a
+    bounded sample: the first S columns of the globe, one step each call."""
+    from gitm_b200 import abi
+    from gitm_b200.parallel import shard_member
+    from oracle import oracle
+
+    threads = threads or os.cpu_count() or 1
+    p = abi.default_params()
+    probe = shard_member(m, 0, max(1, m.n_cols // (64 * threads)))
+    t0 = time.perf_counter()
+    oracle.advance(probe.copy(), p, DT, 1, nthreads=threads)
+    rate = probe.n_cols / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(m.n_cols, max(threads, rate * seconds)))
+    sample = shard_member(m, 0, max(1, m.n_cols // n)) if n < m.n_cols else m.copy()
+    t0 = time.perf_counter()
+    oracle.advance(sample, p, DT, 1, nthreads=threads)
+    el = time.perf_counter() - t0
+    return {"value": sample.n_cols / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample.n_cols} of {m.n_cols} columns x 1 step (nAlts {m.n_alts}), "
+                      f"C++ oracle -O3, {threads} threads, {el:.1f} s"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from gitm_b200 import synthetic
+
+    m = synthetic.globe_member(args.deg, args.deg, n_alts=args.n_alts, seed=0)
+    vals = []
+    per_step = args.cpu_seconds / max(1, args.steps + args.warmup)
+    per_step = max(per_step, 1.0)
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(m, min(per_step, 10.0))
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals) if vals else cb["value"]
+    cb["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * m.n_cols / v,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded)",
+           "config": {"workload": f"globe {args.deg} deg, {m.n_cols} columns x {args.n_alts} alts, "
+                                  "Rusanov RK4, dt 2 s",
+                      "parallelism": "host threads"},
+           "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from gitm_b200 import abi, synthetic
+    from gitm_b200 import vertical as V
+
+    m = synthetic.globe_member(args.deg, args.deg, n_alts=args.n_alts, seed=rank)
+    n_cols = m.n_cols
+    p = abi.default_params()
+    ctx = V.VerticalContext(p, device=local)
+    dm = V.device_member(m, device=dev)
+    plan = V.Plan(ctx, [dm])
+    stream = torch.cuda.current_stream(dev)
+
+    # -- plain per-step drop-in (default launch shape, one synchronous call per step)
+    plain = None
+    if args.plain_steps > 0:
+        V.advance_vertical_all(ctx, [dm], DT, 1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.plain_steps):
+            V.advance_vertical_all(ctx, [dm], DT, 1)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        plain = {"value": n_cols * args.plain_steps / el, "unit": UNIT,
+                 "ms_per_step": 1e3 * el / args.plain_steps,
+                 "how": "gitm_vert_advance_native per step (plan built each call, 256 threads, "
+                        "1 step per launch, synchronous), wall clock"}
+        # restore the input state for the batched run
+        dm = V.device_member(m, device=dev)
+        plan.close()
+        plan = V.Plan(ctx, [dm])
+
+    # -- batched: autotuned launch shape, graph-captured steps
+    if not args.no_autotune:
+        plan.autotune(DT, min(args.steps, 8))
+    cfg = plan.config
+    plan.advance(DT, max(args.warmup, 1), stream=stream)
+    torch.cuda.synchronize()
+    plan.check()
+    graph = torch.cuda.CUDAGraph()
+    cap = torch.cuda.Stream(dev)
+    cap.wait_stream(stream)
+    with torch.cuda.stream(cap):
+        with torch.cuda.graph(graph, stream=cap):
+            plan.advance(DT, args.steps, stream=cap)
+    torch.cuda.synchronize()
+    launches = plan.launch_count(args.steps)
+
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(cap):
+        e0.record(cap)
+        graph.replay()
+        e1.record(cap)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    el = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        t = torch.tensor([el], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+        dist.barrier()
+    st, nbad = plan.status(clear=True)
+    total_cs = n_cols * args.steps * world
+    value = total_cs / el
+
+    # -- end to end through the host-pointer C ABI (pinned host buffers)
+    e2e = None
+    if args.e2e_steps > 0:
+        pinned = m.copy()
+        bufs = {}
+        for name, arr in pinned.arrays():
+            t = torch.from_numpy(arr).pin_memory()
+            bufs[name] = t
+            setattr(pinned, name, t.numpy())
+        h2d = sum(getattr(pinned, k).nbytes for k in ("ndensity_s", "idensity_s", "rho", "temperature",
+                                                        "velocity", "vert_vel", "ivel_up", "eddy",
+                                                        "cos_lat", "sza", "mlat"))
+        d2h = sum(getattr(pinned, k).nbytes for k in ("ndensity_s", "idensity_s", "rho", "temperature",
+                                                        "velocity", "vert_vel", "log_ns", "ndensity",
+                                                        "gamma", "mean_major_mass", "temp_unit", "cmax"))
+        V.advance_vertical_all_host(ctx, [pinned], DT, 1)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            V.advance_vertical_all_host(ctx, [pinned], DT, 1)
+        torch.cuda.synchronize()
+        ee = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([ee], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ee = float(t.item())
+        e2e = {"value": n_cols * args.e2e_steps * world / ee, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "how": "gitm_vert_advance_native_host per step: pinned host arrays copied in, "
+                      "stepped, copied out (chunked, overlapped); wall clock"}
+
+    if rank == 0:
+        flops_cs = opcount(args.n_alts)
+        n_launch = max(1, launches)
+        t_launch = el / n_launch
+        cs_launch = n_cols * args.steps / n_launch
+        fp64_peak = measure_fp64_peak(torch, dev)
+        hbm_peak = None
+        try:
+            hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        except Exception:
+            pass
+        bytes_cs = algorithmic_bytes_per_column_step(args.n_alts) / max(1, cfg.steps_per_launch)
+        achieved = flops_cs * cs_launch / t_launch / 1e12
+        traffic = profile_traffic()
+        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak,
+                "traffic": None if traffic is None else traffic * cs_launch,
+                "kernel": "vert_step_kernel",
+                "peak_source": "FP64 DGEMM (cuBLAS via torch.matmul 8192^3) measured in this run",
+                "flops_per_column_step": flops_cs,
+                "flop_convention": "add/mul/div/sqrt = 1, exp/log/pow = 20 (oracle count, dead code excluded)"}
+        hbm = None
+        if hbm_peak:
+            ach = bytes_cs * n_cols * args.steps / el / 1e9
+            hbm = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                   "frac": ach / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+        cb = cpu_baseline(m, args.cpu_seconds) if args.cpu_seconds > 0 else None
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+               "config": {"workload": f"globe {args.deg} deg, {n_cols} columns x {args.n_alts} alts "
+                                      "per GPU, Rusanov RK4, dt 2 s",
+                          "columns_per_gpu": n_cols, "n_alts": args.n_alts,
+                          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                          "l2": "state larger than L2 (no flush needed)",
+                          "launch": {"threads": cfg.threads, "cols_per_cta": cfg.cols_per_cta,
+                                     "steps_per_launch": cfg.steps_per_launch,
+                                     "ctas_per_sm": cfg.ctas_per_sm, "graph": True}},
+               "clocks": clk, "gpu_launches": launches, "status": {"or": st, "bad_columns": nbad},
+               "roofline": roof, "roofline_hbm": hbm, "cpu_baseline": cb, "e2e": e2e,
+               "plain": plain}
+        print(json.dumps(out))
+    plan.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

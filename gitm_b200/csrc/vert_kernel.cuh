@@ -1,0 +1,896 @@
+// vert_kernel.cuh -- fused RK4 vertical-advance kernel (Rusanov solver).
+//
+// One CTA holds a tile of `nc` columns of one member in shared memory for a
+// whole time step (and for `n_steps` consecutive steps): the gather of
+// advance_vertical (advance_vertical.f90:80-155), the four explicit stages of
+// advance_vertical_1d_rusanov (vertical_solver_rusanov.f90:10-384), the five
+// set_vertical_bcs passes (set_vertical_bcs.Earth.f90:8-652) and the scatter
+// (advance_vertical.f90:163-217) never leave the SM.
+//
+// Thread mapping.  The interior cells of the tile's columns are "items": item
+// t < nc * nAlts owns column t / nAlts, cell t % nAlts + 1, for the whole step
+// (its RK accumulator lives in its registers).  Set_vertical_bcs runs one warp
+// per column with lanes over species / ions.  Whole-column passes (load,
+// store, ghost resets) stride over all threads.
+//
+// Arithmetic is FP64 throughout.  Results agree with the reference's
+// operation order to rounding: reciprocals replace some divisions, the
+// friction matrix is formed without the cancelling NDensity factors, and its
+// 6x6 system (strictly diagonally dominant by rows) is solved by LU without
+// pivoting instead of ludcmp's implicit partial pivoting.
+#pragma once
+
+#include "vert_common.cuh"
+
+namespace gv {
+
+__constant__ Consts c_k;
+
+// DiffExp(i,j) as an index into Consts::one_minus_e; a compile-time table so
+// that fully unrolled loops select the power without indexing registers.
+__device__ __forceinline__ int exp_index(int r, int q) {
+  constexpr int t[NS][NS] = {{0, 0, 0, 0, 1, 2}, {0, 0, 1, 0, 1, 3}, {0, 1, 0, 0, 5, 4},
+                             {0, 0, 0, 0, 0, 4}, {1, 1, 5, 0, 0, 4}, {2, 3, 4, 4, 4, 0}};
+  return t[r][q];
+}
+
+// ------------------------------------------------------------ smem layout
+struct Layout {
+  int nAlts, G;
+  int X, XP, O, OP, LC, DL, TU, CM, GM, SC, stride;
+};
+
+constexpr int NSC = 32;  // per-column scalars
+enum Scalar : int {
+  SC_CENT = 0, SC_CORI = 1, SC_SZA = 2, SC_MLAT = 3, SC_MMM_M1 = 4, SC_MMM_0 = 5,
+  SC_PLASMA = 6, SC_HASLBC = 7, SC_LBC = 8  // 8..27: lbc[2][10]
+};
+
+__host__ __device__ inline Layout make_layout(int nAlts) {
+  Layout L;
+  L.nAlts = nAlts;
+  L.G = nAlts + 4;
+  const int G = L.G;
+  int o = 0;
+  L.X = o;  o += NF * G;
+  L.XP = o; o += NPAS * NPC;
+  L.O = o;  o += NF * G;
+  L.OP = o; o += NPAS * NPC;
+  L.LC = o; o += NS * G;
+  L.DL = o; o += NSTENCIL * (nAlts + 2);
+  L.TU = o; o += G;
+  L.CM = o; o += G;
+  L.GM = o; o += G;
+  L.SC = o; o += NSC;
+  L.stride = o;
+  return L;
+}
+
+// Bytes of dynamic shared memory a tile of nc columns needs.
+__host__ __device__ inline size_t smem_bytes(int nAlts, int nc) {
+  Layout L = make_layout(nAlts);
+  return size_t(L.stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
+}
+
+// passive-ion cell slot: -1,0,1 -> 0..2; nAlts-5..nAlts+2 -> 3..10
+__device__ __forceinline__ int pcell(int i, int nAlts) {
+  return (i <= 1) ? i + 1 : 3 + (i - (nAlts - 5));
+}
+__device__ __forceinline__ bool in_pcells(int i, int nAlts) {
+  return i <= 1 || i >= nAlts - 5;
+}
+
+__device__ __forceinline__ bool photochemical(int s) { return s == 3 || s == 4; }  // N(4S), NO
+
+// ModLimiter.f90:16-36
+__device__ __forceinline__ double limiter_mc(double u, double d, double beta) {
+  if (u > 0.0) {
+    if (d > 0.0) return fmin(fmin(beta * u, beta * d), (u + d) * 0.5);
+    return 0.0;
+  }
+  if (d < 0.0) return fmax(fmax(beta * u, beta * d), (u + d) * 0.5);
+  return 0.0;
+}
+
+struct ColCtx {
+  double* col;
+  Layout L;
+  const double* gridc;
+  int gcols;
+  int gc;  // grid column (0 when the member shares one grid)
+
+  __device__ __forceinline__ double& x(int f, int i) const { return col[L.X + f * L.G + i + 1]; }
+  __device__ __forceinline__ double& o(int f, int i) const { return col[L.O + f * L.G + i + 1]; }
+  __device__ __forceinline__ double& lc(int s, int i) const { return col[L.LC + s * L.G + i + 1]; }
+  __device__ __forceinline__ double& dl(int f, int c) const { return col[L.DL + f * (L.nAlts + 2) + c]; }
+  __device__ __forceinline__ double& sc(int k) const { return col[L.SC + k]; }
+  __device__ __forceinline__ double& cm(int i) const { return col[L.CM + i + 1]; }
+  __device__ __forceinline__ double& tu(int i) const { return col[L.TU + i + 1]; }
+  __device__ __forceinline__ double& gm(int i) const { return col[L.GM + i + 1]; }
+  __device__ __forceinline__ double& ion(int s, int i) const {
+    return (s < NADV) ? col[L.X + (F_I + s) * L.G + i + 1]
+                      : col[L.XP + (s - NADV) * NPC + pcell(i, L.nAlts)];
+  }
+  // grid coefficient k at Fortran cell i
+  __device__ __forceinline__ double g(int k, int i) const {
+    return __ldg(gridc + (size_t(k) * L.G + (i + 1)) * gcols + gc);
+  }
+  __device__ __forceinline__ double bcc(int j) const {
+    return __ldg(gridc + (size_t(NGC) * L.G + j) * gcols + gc);
+  }
+  __device__ __forceinline__ double dAF(int i) const { return g(GC_DALTF, i); }
+  __device__ __forceinline__ double effg(int i) const {
+    return g(GC_GRAV, i) + sc(SC_CENT) * g(GC_R, i);  // Gravity + Centrifugal / InvR
+  }
+};
+
+// Sequential sum over lanes 0..n-1 of v (same order as a Fortran DO loop
+// starting from 0.0); every lane gets the result.
+__device__ __forceinline__ double lane_seq_sum(double v, int n) {
+  double s = 0.0;
+  for (int k = 0; k < n; ++k) s = s + __shfl_sync(0xffffffffu, v, k);
+  return s;
+}
+
+// ------------------------------------------------------------ boundaries
+// set_vertical_bcs (Earth), set_vertical_bcs.Earth.f90:8-652, for one column,
+// executed by one full warp.  IVel ghosts and the electron slot are not set:
+// nothing on the path reads them.
+__device__ void bc_column(const ColCtx& c, const GitmVertParams& prm, int lane, uint32_t* st) {
+  const int nA = c.L.nAlts;
+  const bool msis = prm.use_msis_bcs && c.sc(SC_HASLBC) != 0.0;
+  const bool improved = prm.use_improved_ion_advection != 0;
+  const int s = lane;
+
+  // NS(0) and NS(nAlts) as exp(LogNS) on entry (line 93, before the MSIS
+  // values overwrite cell 0)
+  double nsb = 0.0, nst = 0.0;
+  if (s < NS) {
+    nsb = exp(c.x(F_LNS + s, 0));
+    nst = exp(c.x(F_LNS + s, nA));
+  }
+  __syncwarp();
+  // lines 112-148
+  if (msis) {
+    const double* t = &c.col[c.L.SC + SC_LBC];
+    if (s < NS) {
+      c.x(F_LNS + s, -1) = t[s];
+      c.x(F_LNS + s, 0) = t[10 + s];
+    } else if (s == 6) {
+      c.x(F_T, -1) = t[6];
+      c.x(F_T, 0) = t[16];
+    } else if (s == 7) {
+      c.x(F_LRHO, -1) = t[7];
+      c.x(F_LRHO, 0) = t[17];
+    } else if (s == 8) {
+      c.x(F_VE, -1) = t[8];
+      c.x(F_VE, 0) = t[18];
+    } else if (s == 9) {
+      c.x(F_VN, -1) = t[9];
+      c.x(F_VN, 0) = t[19];
+    }
+  } else {
+    if (s == 8) { c.x(F_VE, -1) = 0.0; c.x(F_VE, 0) = 0.0; }
+    if (s == 9) { c.x(F_VN, -1) = 0.0; c.x(F_VN, 0) = 0.0; }
+  }
+  if (s == 10) { c.x(F_VU, -1) = 0.0; c.x(F_VU, 0) = 0.0; }
+  if (s < NS) { c.x(F_W + s, -1) = 0.0; c.x(F_W + s, 0) = 0.0; }
+  __syncwarp();
+  // lines 192-196
+  if (s == 0) {
+    c.x(F_T, -1) = c.x(F_T, 0);
+    c.x(F_VE, -1) = c.x(F_VE, 0);
+    c.x(F_VN, -1) = c.x(F_VN, 0);
+    c.x(F_VU, -1) = c.x(F_VU, 0);
+  }
+  __syncwarp();
+  // lines 198-275: species at cell -1 (hydrostatic) / 0,-1 (photochemical)
+  if (s < NS) {
+    if (!photochemical(s)) {
+      double MeanGravity = -0.5 * (c.effg(-1) + c.effg(0));
+      double MeanTemp = 0.5 * (c.x(F_T, 0) + c.x(F_T, -1));
+      double MeanMass = 0.5 * (c.sc(SC_MMM_0) + c.sc(SC_MMM_M1));
+      double ish = MeanGravity * MeanMass / (MeanTemp * KB);
+      double ns = nsb * (c.x(F_T, 0) / c.x(F_T, -1)) * exp(ish * c.dAF(-1));
+      c.x(F_LNS + s, -1) = (s == 0) ? c.x(F_LNS + s, 0) : log(ns);
+    } else {
+      for (int k = 0; k < 2; ++k) {
+        const int i = -k;
+        double d = c.x(F_LNS + s, i + 1) * c.bcc(k * 5 + 0) + c.x(F_LNS + s, i + 2) * c.bcc(k * 5 + 1) +
+                   c.x(F_LNS + s, i + 3) * c.bcc(k * 5 + 2) + c.x(F_LNS + s, i + 4) * c.bcc(k * 5 + 3) +
+                   c.x(F_LNS + s, i + 5) * c.bcc(k * 5 + 4);
+        double up = c.x(F_LNS + s, i + 1);
+        double v = up - c.dAF(i + 1) * d;
+        if (d <= 0.0) v = up;
+        if (s == 4 && v < up - 0.333) v = up - 0.333;
+        c.x(F_LNS + s, i) = v;
+      }
+    }
+  }
+  // ions float at the lower boundary (lines 304-310)
+  if (s < NI) {
+    c.ion(s, 0) = c.ion(s, 1);
+    c.ion(s, -1) = c.ion(s, 0);
+  }
+  // vertical winds, 3rd-order extrapolation (lines 334-344)
+  if (s < NS) {
+    for (int k = 0; k < 2; ++k) {
+      const int i = -k;
+      double d = c.x(F_W + s, i + 1) * c.bcc(k * 5 + 0) + c.x(F_W + s, i + 2) * c.bcc(k * 5 + 1) +
+                 c.x(F_W + s, i + 3) * c.bcc(k * 5 + 2) + c.x(F_W + s, i + 4) * c.bcc(k * 5 + 3) +
+                 c.x(F_W + s, i + 5) * c.bcc(k * 5 + 4);
+      c.x(F_W + s, i) = c.x(F_W + s, i + 1) - c.dAF(i + 1) * d;
+    }
+  }
+  __syncwarp();
+  // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1
+  for (int k = 0; k < 2; ++k) {
+    const int i = -k;
+    double ns = 0.0, term = 0.0;
+    if (s < NS) {
+      ns = exp(c.x(F_LNS + s, i));
+      term = c_k.mass[s] * ns;
+    }
+    const double SumRho = lane_seq_sum(term, NS);
+    const double lr = log(SumRho);
+    const double er = exp(lr);
+    double t2 = 0.0;
+    if (s < NS) t2 = ns * c_k.mass[s] * c.x(F_W + s, i) / er;
+    const double vu = lane_seq_sum(t2, NS);
+    if (s == 0) {
+      c.x(F_LRHO, i) = lr;
+      c.x(F_VU, i) = vu;
+    }
+  }
+  // lines 364-376
+  if (msis && (s == 8 || s == 9)) {
+    const int f = (s == 8) ? F_VE : F_VN;
+    const int i = -1;
+    double d = c.x(f, i + 1) * c.bcc(5) + c.x(f, i + 2) * c.bcc(6) + c.x(f, i + 3) * c.bcc(7) +
+               c.x(f, i + 4) * c.bcc(8) + c.x(f, i + 5) * c.bcc(9);
+    c.x(f, i) = c.x(f, i + 1) - c.dAF(i + 1) * d;
+  }
+  __syncwarp();
+  // lines 382-395
+  if (s < NS && photochemical(s) && c.x(F_W + s, 1) > 0.0) {
+    c.x(F_W + s, 0) = -1.0 * c.x(F_W + s, 1);
+    c.x(F_W + s, -1) = -1.0 * c.x(F_W + s, 1);
+  }
+
+  // ---- top, lines 420-463
+  if (s == 8) { c.x(F_VE, nA + 1) = c.x(F_VE, nA); c.x(F_VE, nA + 2) = c.x(F_VE, nA); }
+  if (s == 9) { c.x(F_VN, nA + 1) = c.x(F_VN, nA); c.x(F_VN, nA + 2) = c.x(F_VN, nA); }
+  if (s < NS) {
+    double wn = c.x(F_W + s, nA);
+    double w1 = wn, w2 = wn;
+    if (photochemical(s) && wn < 0.0) {
+      w1 = -wn;
+      w2 = -c.x(F_W + s, nA - 1);
+    }
+    c.x(F_W + s, nA + 1) = w1;
+    c.x(F_W + s, nA + 2) = w2;
+  }
+  if (s == 10) {
+    double v = c.x(F_VU, nA);
+    double w = (v < 0.0) ? -v : v;
+    c.x(F_VU, nA + 1) = w;
+    c.x(F_VU, nA + 2) = w;
+  }
+  if (s == 11) {
+    c.x(F_T, nA + 1) = c.x(F_T, nA);
+    c.x(F_T, nA + 2) = c.x(F_T, nA);
+  }
+  __syncwarp();
+  // lines 471-486: hydrostatic neutrals
+  if (s < NS) {
+    double ns = nst;
+    for (int i = nA + 1; i <= nA + 2; ++i) {
+      double MeanGravity = -0.5 * (c.effg(i) + c.effg(i - 1));
+      double MeanTemp = 0.5 * (c.x(F_T, i - 1) + c.x(F_T, i));
+      double ish = MeanGravity * c_k.mass[s] / (MeanTemp * KB);
+      ns = ns * (c.x(F_T, i - 1) / c.x(F_T, i)) * exp(-ish * c.dAF(i));
+      c.x(F_LNS + s, i) = log(ns);
+    }
+  }
+  // lines 497-501: TEC of the first ion
+  double tp = 0.0;
+  for (int i = 1 + lane; i <= nA; i += 32) {
+    double v = c.ion(0, i);
+    tp += c.dAF(i) * (improved ? v : exp(v));
+  }
+  for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
+  const double tec = tp / 1e16;
+  const bool hold = (tec < prm.min_tec) && (c.sc(SC_PLASMA) != 0.0);
+  // lines 503-596: ions at the top
+  if (s < NI) {
+    for (int k = 0; k < 2; ++k) {
+      const int iAlt = nA + 1 + k;
+      double n[6];
+      if (improved) {
+        // check_for_negative_densities, lines 608-649
+        double mn = c.ion(s, iAlt - 5);
+        for (int q = iAlt - 4; q <= iAlt; ++q) mn = fmin(mn, c.ion(s, q));
+        if (mn < 0.0) {
+          if (c.ion(s, iAlt - 6) < 0.0) atomicOr(st, GITM_ST_NEG_ION_TOP);
+          for (int q = iAlt - 5; q <= iAlt - 1; ++q) {
+            if (c.ion(s, q) < 0.0) {
+              if (c.ion(s, q - 1) > 0.0 && c.ion(s, q + 1) > 0.0)
+                c.ion(s, q) = (c.ion(s, q - 1) + c.ion(s, q + 1)) / 2.0;
+              else
+                c.ion(s, q) = c.ion(s, q - 1) * 0.95;
+            }
+          }
+          if (c.ion(s, iAlt) < 0.0) c.ion(s, iAlt) = c.ion(s, iAlt - 1) * 0.95;
+        }
+        for (int j = 0; j < 6; ++j) n[j] = log(c.ion(s, iAlt - j));
+      } else {
+        for (int j = 0; j < 6; ++j) n[j] = c.ion(s, iAlt - j);
+      }
+      double dn = c.bcc(10 + 5 * k + 0) * n[1] + c.bcc(10 + 5 * k + 1) * n[2] +
+                  c.bcc(10 + 5 * k + 2) * n[3] + c.bcc(10 + 5 * k + 3) * n[4] +
+                  c.bcc(10 + 5 * k + 4) * n[5];
+      if (!hold) {
+        const double lim = -(0.001 * n[0] / c.dAF(nA));
+        if (dn > lim) dn = lim;
+        const double n0 = n[1] + dn * c.dAF(iAlt);
+        c.ion(s, iAlt) = improved ? exp(n0) : n0;
+      }
+    }
+  }
+  __syncwarp();
+  // lines 598-604
+  for (int i = nA + 1; i <= nA + 2; ++i) {
+    double term = (s < NS) ? c_k.mass[s] * exp(c.x(F_LNS + s, i)) : 0.0;
+    double SumRho = lane_seq_sum(term, NS);
+    if (s == 0) c.x(F_LRHO, i) = log(SumRho);
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------ the kernel
+struct KParams {
+  const DevMember* members;
+  const Tile* tiles;
+  int n_tiles;
+  int n_steps;
+  double dt;
+  uint32_t* status;  // one word per column (member col_offset + column)
+  GitmVertParams prm;
+};
+
+constexpr double F1 = 0.6250000;  // Factor1, vertical_solver_rusanov.f90:739
+constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
+
+// IO = 0: GITM arrays (advance_vertical gather/scatter);
+// IO = 1: ModVertical arrays (advance_vertical_1d_* arguments).
+template <int IO, int NT>
+__global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
+  extern __shared__ double sm[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const GitmVertParams& prm = kp.prm;
+  const double dt = kp.dt;
+
+  for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
+    const Tile tile = kp.tiles[tix];
+    const DevMember& M = kp.members[tile.member];
+    const int nA = M.b.n_alts;
+    const int nc = tile.nc;
+    const Layout L = make_layout(nA);
+    const int G = L.G;
+    const int64_t ncols = M.b.n_cols;
+    uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(L.stride) * nc);  // [nc] status
+    uint32_t* sfrozen = sst + nc;                                             // [nc]
+    const int nitems = nc * nA;
+    const bool item = tid < nitems;
+    const int my_cl = item ? tid / nA : 0;
+    const int my_i = item ? tid % nA + 1 : 1;
+
+    auto ctx = [&](int cl) {
+      ColCtx c;
+      c.col = sm + size_t(L.stride) * cl;
+      c.L = L;
+      c.gridc = M.gridc;
+      c.gcols = M.gcols;
+      c.gc = (M.gcols == 1) ? 0 : int(tile.c0 + cl);
+      return c;
+    };
+    auto gidx = [&](int f, int g, int cl) -> int64_t {
+      return (int64_t(f) * G + g) * ncols + tile.c0 + cl;
+    };
+
+    if (tid < nc) {
+      sst[tid] = 0u;
+      sfrozen[tid] = 0u;
+    }
+    __syncthreads();
+
+    // ---------------------------------------------------------- load
+    // per-column scalars (advance_vertical.f90:84-85,103-104)
+    if (tid < nc) {
+      ColCtx c = ctx(tid);
+      const int64_t cc = tile.c0 + tid;
+      double cent, cori, sza, mlat;
+      if (IO == 0) {
+        const double cl = M.b.cos_lat[cc];
+        cent = (cl * prm.omega_body) * (cl * prm.omega_body);
+        cori = 2 * cl * prm.omega_body;
+        sza = M.b.sza[cc];
+        mlat = M.b.mlat[cc];
+      } else {
+        cent = M.mv.centrifugal[cc];
+        cori = M.mv.coriolis[cc];
+        sza = M.mv.sza[cc];
+        mlat = M.mv.mlat[cc];
+      }
+      c.sc(SC_CENT) = cent;
+      c.sc(SC_CORI) = cori;
+      c.sc(SC_SZA) = sza;
+      c.sc(SC_MLAT) = mlat;
+      // set_vertical_bcs.Earth.f90:488-495
+      bool plasma = false;
+      if (prm.use_nighttime_ion_bcs)
+        plasma = sza > PI / 2 && ((mlat > 30.0 && mlat < 70.0) || (mlat > -60.0 && mlat < -30.0));
+      c.sc(SC_PLASMA) = plasma ? 1.0 : 0.0;
+      const double* lbc = (IO == 0) ? M.b.lbc : M.mv.lbc;
+      c.sc(SC_HASLBC) = lbc ? 1.0 : 0.0;
+      if (lbc)
+        for (int k = 0; k < 2 * GITM_LBC_NVALUES; ++k)
+          c.sc(SC_LBC + k) = lbc[int64_t(k) * ncols + cc];
+    }
+    for (int w = tid; w < nc * G; w += NT) {
+      const int cl = w / G, g = w - cl * G, i = g - 1;
+      ColCtx c = ctx(cl);
+      if (IO == 0) {
+        const GitmColumnBatch& b = M.b;
+        double nd[NS], ww[NS];
+        double mn = 1.0;
+        for (int s = 0; s < NS; ++s) {
+          nd[s] = b.ndensity_s[gidx(s, g, cl)];
+          ww[s] = b.vert_vel[gidx(s, g, cl)];
+          mn = fmin(mn, nd[s]);
+        }
+        if (!(mn > 0.0)) atomicOr(&sfrozen[cl], 1u);
+        const double temperature = b.temperature[gidx(0, g, cl)];
+        double gamma, mmm, tu, cmx = 0.0;
+        if (prm.compute_coefficients) {
+          // calc_pressure.f90:17-21,56-83; calc_rates.Earth.f90:34-50;
+          // calc_timestep.f90:114-118
+          double N = 0.0;
+          for (int s = 0; s < NS; ++s) N = N + nd[s];
+          double gg = 0.0;
+          for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
+          gamma = gg * 2.0 / N + 1;
+          double m = 0.0;
+          const double rn = 1.0 / (N + 1.0);
+          for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
+          if (m == 0) m = c_k.mass[0];
+          mmm = m;
+          tu = m * (1.0 / KB);
+          if (g >= 1 && g <= nA + 2) {
+            double mx = fabs(ww[0]);
+            for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(ww[s]));
+            cmx = mx + sqrt(gamma * temperature);
+          }
+          if (kp.n_steps == 1) {
+            if (b.gamma) b.gamma[gidx(0, g, cl)] = gamma;
+            if (b.mean_major_mass) b.mean_major_mass[gidx(0, g, cl)] = mmm;
+            if (b.temp_unit) b.temp_unit[gidx(0, g, cl)] = tu;
+            if (b.cmax && g >= 1 && g <= nA + 2) b.cmax[gidx(0, g, cl)] = cmx;
+          }
+        } else {
+          gamma = b.gamma[gidx(0, g, cl)];
+          mmm = b.mean_major_mass[gidx(0, g, cl)];
+          tu = b.temp_unit[gidx(0, g, cl)];
+          if (g >= 1 && g <= nA + 2) cmx = b.cmax[gidx(0, g, cl)];
+        }
+        c.tu(i) = tu;
+        c.cm(i) = cmx;
+        c.gm(i) = gamma;
+        if (i == -1) c.sc(SC_MMM_M1) = mmm;
+        if (i == 0) c.sc(SC_MMM_0) = mmm;
+        for (int s = 0; s < NS; ++s) {
+          c.x(F_LNS + s, i) = log(nd[s]);
+          c.x(F_W + s, i) = ww[s];
+        }
+        c.x(F_T, i) = temperature * tu;
+        c.x(F_VE, i) = b.velocity[gidx(0, g, cl)];
+        c.x(F_VN, i) = b.velocity[gidx(1, g, cl)];
+        c.x(F_VU, i) = b.velocity[gidx(2, g, cl)];
+        c.x(F_LRHO, i) = log(b.rho[gidx(0, g, cl)]);
+        const bool pc = in_pcells(i, nA);
+        for (int s = 0; s < NI; ++s) {
+          if (s >= NADV && !pc) continue;
+          const double v = b.idensity_s[gidx(s, g, cl)];
+          c.ion(s, i) = prm.use_improved_ion_advection ? v : log(v);
+        }
+      } else {
+        const GitmModVerticalBatch& b = M.mv;
+        for (int s = 0; s < NS; ++s) {
+          c.x(F_LNS + s, i) = b.log_ns[gidx(s, g, cl)];
+          c.x(F_W + s, i) = b.vert_vel[gidx(s, g, cl)];
+        }
+        c.x(F_T, i) = b.temp[gidx(0, g, cl)];
+        c.x(F_VE, i) = b.vel_gd[gidx(0, g, cl)];
+        c.x(F_VN, i) = b.vel_gd[gidx(1, g, cl)];
+        c.x(F_VU, i) = b.vel_gd[gidx(2, g, cl)];
+        c.x(F_LRHO, i) = b.log_rho[gidx(0, g, cl)];
+        const bool pc = in_pcells(i, nA);
+        for (int s = 0; s < NI; ++s) {
+          if (s >= NADV && !pc) continue;
+          c.ion(s, i) = b.log_ins[gidx(s, g, cl)];
+        }
+        c.cm(i) = (g >= 1 && g <= nA + 2) ? b.cmax[gidx(0, g, cl)] : 0.0;
+        c.gm(i) = b.gamma[gidx(0, g, cl)];
+        c.tu(i) = 1.0;
+        if (i == -1) c.sc(SC_MMM_M1) = b.mean_major_mass[gidx(0, g, cl)];
+        if (i == 0) c.sc(SC_MMM_0) = b.mean_major_mass[gidx(0, g, cl)];
+      }
+    }
+    __syncthreads();
+
+    // per-item constants for the step
+    double eddy = 0.0, ivup = 0.0;
+    double acc[NF];
+
+    for (int step = 0; step < kp.n_steps; ++step) {
+      if (item) {
+        if (IO == 0) {
+          eddy = M.b.eddy[gidx(0, my_i + 1, my_cl)];
+          ivup = M.b.ivel_up[gidx(0, my_i + 1, my_cl)];
+        } else {
+          eddy = M.mv.eddy[gidx(0, my_i + 1, my_cl)];
+          ivup = M.mv.ivel[gidx(2, my_i + 1, my_cl)];
+        }
+      }
+      // ---------------------------------------------------- first BC pass
+      if (wid < nc) bc_column(ctx(wid), prm, lane, &sst[wid]);
+      __syncthreads();
+      // Orig = state (vertical_solver_rusanov.f90:95-100)
+      for (int w = tid; w < nc * (NF * G + NPAS * NPC); w += NT) {
+        const int per = NF * G + NPAS * NPC;
+        const int cl = w / per, r = w - cl * per;
+        double* col = sm + size_t(L.stride) * cl;
+        if (r < NF * G)
+          col[L.O + r] = col[L.X + r];
+        else
+          col[L.OP + r - NF * G] = col[L.XP + r - NF * G];
+      }
+      // no barrier needed here: the stage below reads X only until its
+      // first barrier, and Orig is first read after it
+
+      for (int k = 0; k < 4; ++k) {
+        // -------------------------------------------------- phase A
+        // LogConS on every cell (vertical_solver_rusanov.f90:506-509) and the
+        // limited slopes of the 18 swept fields on cells 0..nAlts+1
+        // (calc_facevalues_alts_rusanov, :745-772).
+        double ns[NS], rho = 1.0;
+        if (item) {
+          ColCtx c = ctx(my_cl);
+          const int i = my_i;
+          rho = exp(c.x(F_LRHO, i));
+          const double ir = 1.0 / rho;
+          for (int s = 0; s < NS; ++s) {
+            ns[s] = exp(c.x(F_LNS + s, i));
+            c.lc(s, i) = log(c_k.mass[s] * ns[s] * ir);
+          }
+          const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+#pragma unroll 2
+          for (int f = 0; f < NSTENCIL; ++f) {
+            const double* v = &c.col[L.X + f * G + 1];
+            const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+            const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
+            c.dl(f, i) = limiter_mc(up, dn, prm.beta_limiter);
+          }
+        }
+        // extra units: LogConS of the 4 ghost cells and the two end slopes
+        for (int q = tid - nitems; q < nc * 6; q += NT) {
+          if (q < 0) continue;
+          const int cl = q / 6, u = q - cl * 6;
+          ColCtx c = ctx(cl);
+          if (u < 4) {
+            const int i = (u < 2) ? u - 1 : nA + u - 1;  // -1, 0, nA+1, nA+2
+            const double ir = 1.0 / exp(c.x(F_LRHO, i));
+            for (int s = 0; s < NS; ++s) c.lc(s, i) = log(c_k.mass[s] * exp(c.x(F_LNS + s, i)) * ir);
+          } else {
+            const int i = (u == 4) ? 0 : nA + 1;
+            const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+            for (int f = 0; f < NSTENCIL; ++f) {
+              const double* v = &c.col[L.X + f * G + 1];
+              c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, prm.beta_limiter);
+            }
+          }
+        }
+        __syncthreads();
+
+        // -------------------------------------------------- phase B
+        double kv[NF];
+        if (item) {
+          ColCtx c = ctx(my_cl);
+          const int i = my_i;
+          const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
+          const double idc = c.g(GC_IDC, i);
+          const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
+          const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
+          // calc_rusanov_alts_rusanov (:694-718) at cell i
+          auto sweep = [&](int f, double& grad, double& diff) {
+            const double* v = &c.col[L.X + f * G + 1];
+            const double* d = &c.col[L.DL + f * (nA + 2)];
+            const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
+            const double R0 = v[i] - 0.5 * d[i] * dF0;
+            const double L1 = v[i] + 0.5 * d[i] * dF1;
+            const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
+            grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+            diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
+          };
+          const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
+          const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
+          double gT, dT, gE, dE, gN, dN, gU, dU;
+          sweep(F_T, gT, dT);
+          sweep(F_VE, gE, dE);
+          sweep(F_VN, gN, dN);
+          sweep(F_VU, gU, dU);
+          // :660-680
+          kv[F_VE] = (VE - dt * VU * gE + dt * dE) - VE;
+          kv[F_VN] = (VN - dt * VU * gN + dt * dN) - VN;
+          const double divv = gU + 2 * VU * invr;
+          kv[F_T] = (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T;
+          // ions 1..nIonsAdvect (:557-568)
+          for (int s = 0; s < NADV; ++s) {
+            double gI, dI;
+            sweep(F_I + s, gI, dI);
+            const double I = c.x(F_I + s, i);
+            kv[F_I + s] = (I - dt * (ivup * gI) + dt * dI) - I;
+          }
+          // species continuity and momentum (:548-617)
+          const double tau = prm.use_damping
+                                 ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
+                                 : prm.vert_tau;
+          const double hz = (VN * VN + VE * VE) * invr;
+          const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
+          double wv[NS];
+          double sumrho = 0.0;
+          for (int s = 0; s < NS; ++s) {
+            double gL, dL, gW, dW;
+            sweep(F_LNS + s, gL, dL);
+            sweep(F_W + s, gW, dW);
+            const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
+            const double divw = gW + 2 * Ws * invr;
+            const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
+            kv[F_LNS + s] = nl - Ls;
+            sumrho = sumrho + c_k.mass[s] * exp(nl);
+            const double km = c_k.k_over_m[s];
+            double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws / tau;
+            w = w + cor;
+            w = w - dt * (prm.thermal_diff_coef[s] * KB * gT) / c_k.mass[s];
+            wv[s] = w;
+          }
+          kv[F_LRHO] = log(sumrho) - c.x(F_LRHO, i);
+          // calc_neutral_friction (calc_neutral_friction.f90:47-106)
+          if (prm.use_neutral_friction) {
+            double glc[NS];
+            const double m0 = c.g(GC_M0 + 0, i), m1 = c.g(GC_M0 + 1, i), m2 = c.g(GC_M0 + 2, i),
+                         m3 = c.g(GC_M0 + 3, i), m4 = c.g(GC_M0 + 4, i);
+            for (int s = 0; s < NS; ++s)
+              glc[s] = m0 * c.lc(s, i - 2) + m1 * c.lc(s, i - 1) + m2 * c.lc(s, i) +
+                       m3 * c.lc(s, i + 1) + m4 * c.lc(s, i + 2);
+            const double lt = log(T);
+            double pw[NS];
+#pragma unroll
+            for (int e = 0; e < NS; ++e) pw[e] = exp(c_k.one_minus_e[e] * lt);
+            double a[NS][NS];
+#pragma unroll
+            for (int r = 0; r < NS; ++r) {
+              double rs = 0.0;
+#pragma unroll
+              for (int q = 0; q < NS; ++q) {
+                if (q == r) continue;
+                const double cij = c_k.kc[r][q] * ns[q] * pw[exp_index(r, q)];
+                a[r][q] = -dt * cij;
+                rs = rs + cij;
+              }
+              a[r][r] = 1.0 + dt * rs;
+            }
+            // LU without pivoting (the matrix is strictly row diagonally dominant)
+#pragma unroll
+            for (int p = 0; p < NS; ++p) {
+              const double ip = 1.0 / a[p][p];
+              a[p][p] = ip;
+#pragma unroll
+              for (int r = p + 1; r < NS; ++r) {
+                const double l = a[r][p] * ip;
+#pragma unroll
+                for (int q = p + 1; q < NS; ++q) a[r][q] -= l * a[p][q];
+                wv[r] -= l * wv[p];
+              }
+            }
+#pragma unroll
+            for (int r = NS - 1; r >= 0; --r) {
+              double sum = wv[r];
+#pragma unroll
+              for (int q = r + 1; q < NS; ++q) sum -= a[r][q] * wv[q];
+              wv[r] = sum * a[r][r];
+            }
+            for (int s = 0; s < NS; ++s) wv[s] = wv[s] + (-eddy * glc[s]);
+          }
+          // clamp and bulk vertical wind (:643-658)
+          const double ir = 1.0 / rho;
+          double vu = 0.0;
+          for (int s = 0; s < NS; ++s) {
+            double w = fmax(-prm.max_vertical_velocity, wv[s]);
+            w = fmin(prm.max_vertical_velocity, w);
+            kv[F_W + s] = w - c.x(F_W + s, i);
+            vu = vu + w * (c_k.mass[s] * ns[s] * ir);
+          }
+          kv[F_VU] = vu - VU;
+        }
+        __syncthreads();
+
+        // -------------------------------------------------- RK update
+        // vertical_solver_rusanov.f90:120-163,190-232,261-303,330-366
+        if (item) {
+          ColCtx c = ctx(my_cl);
+          const int i = my_i;
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            if (k == 0) acc[f] = kv[f];
+            else if (k < 3) acc[f] = acc[f] + 2.0 * kv[f];
+            else acc[f] = acc[f] + kv[f];
+            const double o = c.o(f, i);
+            c.x(f, i) = (k < 2) ? o + 0.5 * kv[f] : (k == 2) ? o + kv[f] : o + (1.0 / 6.0) * acc[f];
+          }
+        }
+        // ghost cells and passive ions return to Orig (their K is zero)
+        for (int w = tid; w < nc * (NF * 4 + NPAS * NPC); w += NT) {
+          const int per = NF * 4 + NPAS * NPC;
+          const int cl = w / per, r = w - cl * per;
+          double* col = sm + size_t(L.stride) * cl;
+          if (r < NF * 4) {
+            const int f = r >> 2, u = r & 3;
+            const int g = (u < 2) ? u : nA + u;  // cells -1,0,nA+1,nA+2
+            col[L.X + f * G + g] = col[L.O + f * G + g];
+          } else {
+            col[L.XP + r - NF * 4] = col[L.OP + r - NF * 4];
+          }
+        }
+        __syncthreads();
+        if (k < 3) {
+          if (wid < nc) bc_column(ctx(wid), prm, lane, &sst[wid]);
+          __syncthreads();
+        }
+      }
+      // final set_vertical_bcs (:368-369)
+      if (wid < nc) bc_column(ctx(wid), prm, lane, &sst[wid]);
+      __syncthreads();
+
+      // ---------------------------------------------------- store / reload
+      const bool last = (step == kp.n_steps - 1);
+      for (int w = tid; w < nc * G; w += NT) {
+        const int cl = w / G, g = w - cl * G, i = g - 1;
+        ColCtx c = ctx(cl);
+        const bool store = last && sfrozen[cl] == 0u;
+        if (IO == 1) {
+          if (!store) continue;
+          const GitmModVerticalBatch& b = M.mv;
+          for (int s = 0; s < NS; ++s) {
+            b.log_ns[gidx(s, g, cl)] = c.x(F_LNS + s, i);
+            b.vert_vel[gidx(s, g, cl)] = c.x(F_W + s, i);
+          }
+          b.temp[gidx(0, g, cl)] = c.x(F_T, i);
+          b.vel_gd[gidx(0, g, cl)] = c.x(F_VE, i);
+          b.vel_gd[gidx(1, g, cl)] = c.x(F_VN, i);
+          b.vel_gd[gidx(2, g, cl)] = c.x(F_VU, i);
+          b.log_rho[gidx(0, g, cl)] = c.x(F_LRHO, i);
+          const bool pc = in_pcells(i, nA);
+          for (int s = 0; s < NI; ++s)
+            if (s < NADV || pc) b.log_ins[gidx(s, g, cl)] = c.ion(s, i);
+          continue;
+        }
+        // scatter, advance_vertical.f90:163-217
+        const GitmColumnBatch& b = M.b;
+        const double rho = exp(c.x(F_LRHO, i));
+        const double temperature = c.x(F_T, i) / c.tu(i);
+        double nd[NS], N = 0.0;
+        bool finite = isfinite(rho) && isfinite(temperature);
+        for (int s = 0; s < NS; ++s) {
+          nd[s] = exp(c.x(F_LNS + s, i));
+          N = N + nd[s];
+          finite = finite && isfinite(nd[s]) && isfinite(c.x(F_W + s, i));
+        }
+        const bool improved = prm.use_improved_ion_advection != 0;
+        const bool pc = in_pcells(i, nA);
+        const bool interior = (i >= 1 && i <= nA);
+        if (store) {
+          b.rho[gidx(0, g, cl)] = rho;
+          b.velocity[gidx(0, g, cl)] = c.x(F_VE, i);
+          b.velocity[gidx(1, g, cl)] = c.x(F_VN, i);
+          b.velocity[gidx(2, g, cl)] = c.x(F_VU, i);
+          b.temperature[gidx(0, g, cl)] = temperature;
+          for (int s = 0; s < NS; ++s) {
+            if (b.log_ns) b.log_ns[gidx(s, g, cl)] = c.x(F_LNS + s, i);
+            b.vert_vel[gidx(s, g, cl)] = c.x(F_W + s, i);
+            b.ndensity_s[gidx(s, g, cl)] = nd[s];
+          }
+          if (b.ndensity) b.ndensity[gidx(0, g, cl)] = N;
+          if (prm.use_ion_advection) {
+            double e = 0.0;
+            for (int s = 0; s < NI; ++s) {
+              double v;
+              if (s < NADV || pc) {
+                v = c.ion(s, i);
+                if (!improved) v = exp(v);
+              } else {
+                v = b.idensity_s[gidx(s, g, cl)];  // unchanged interior value
+              }
+              if (improved && interior && v < 1) v = 1.0;
+              finite = finite && isfinite(v);
+              if (s < NADV || pc || v != b.idensity_s[gidx(s, g, cl)]) b.idensity_s[gidx(s, g, cl)] = v;
+              e = e + v;
+            }
+            b.idensity_s[gidx(NI, g, cl)] = e;
+          }
+          if (!finite) atomicOr(&sst[cl], GITM_ST_NONFINITE);
+        }
+        if (!last) {
+          // the next step's gather from the values just formed
+          double gamma = c.gm(i), mmm = 0.0, tu = c.tu(i), cmx = c.cm(i);
+          bool bad = false;
+          for (int s = 0; s < NS; ++s) bad = bad || !(nd[s] > 0.0);
+          if (bad) atomicOr(&sst[cl], GITM_ST_NEG_DENSITY);
+          if (prm.compute_coefficients) {
+            double gg = 0.0;
+            for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
+            gamma = gg * 2.0 / N + 1;
+            double m = 0.0;
+            const double rn = 1.0 / (N + 1.0);
+            for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
+            if (m == 0) m = c_k.mass[0];
+            mmm = m;
+            tu = m * (1.0 / KB);
+            cmx = 0.0;
+            if (g >= 1 && g <= nA + 2) {
+              double mx = fabs(c.x(F_W, i));
+              for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(c.x(F_W + s, i)));
+              cmx = mx + sqrt(gamma * temperature);
+            }
+            if (step + 1 == kp.n_steps - 1) {
+              if (b.gamma) b.gamma[gidx(0, g, cl)] = gamma;
+              if (b.mean_major_mass) b.mean_major_mass[gidx(0, g, cl)] = mmm;
+              if (b.temp_unit) b.temp_unit[gidx(0, g, cl)] = tu;
+              if (b.cmax && g >= 1 && g <= nA + 2) b.cmax[gidx(0, g, cl)] = cmx;
+            }
+            c.gm(i) = gamma;
+            c.cm(i) = cmx;
+            c.tu(i) = tu;
+            if (i == -1) c.sc(SC_MMM_M1) = mmm;
+            if (i == 0) c.sc(SC_MMM_0) = mmm;
+          }
+          for (int s = 0; s < NS; ++s) c.x(F_LNS + s, i) = log(nd[s]);
+          c.x(F_T, i) = temperature * tu;
+          c.x(F_LRHO, i) = log(rho);
+          if (prm.use_ion_advection) {
+            for (int s = 0; s < NI; ++s) {
+              if (!(s < NADV || pc)) continue;
+              double v = c.ion(s, i);
+              if (!improved) v = exp(v);
+              if (improved && interior && v < 1) v = 1.0;
+              c.ion(s, i) = improved ? v : log(v);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    if (tid < nc) {
+      const int64_t gcol = M.col_offset + tile.c0 + tid;
+      uint32_t w = sst[tid];
+      if (sfrozen[tid]) w |= GITM_ST_NEG_DENSITY;
+      if (w) kp.status[gcol] |= w;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace gv

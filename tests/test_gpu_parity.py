@@ -1,0 +1,233 @@
+"""CUDA path vs the CPU oracle on identical seeded inputs (run on a B200).
+
+Every call goes through libgitmvert.so (the C ABI); see tests/parity.py for
+the tolerance.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from gitm_b200 import abi, synthetic
+from tests.parity import RTOL, assert_state_close
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+STATE = synthetic.Member.STATE + ("log_ns", "ndensity")
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def gpu_advance(m, params, dt, n_steps=1, config=None):
+    from gitm_b200 import vertical as V
+    ctx = V.VerticalContext(params)
+    dm = V.device_member(m)
+    plan = V.Plan(ctx, [dm])
+    if config:
+        plan.set_config(**config)
+    plan.advance(dt, n_steps)
+    words = plan.status_words()
+    out = dm.to_numpy()
+    plan.close()
+    ctx.close()
+    return out, words
+
+
+def ref_advance(oracle_lib, m, params, dt, n_steps=1):
+    r = m.copy()
+    st = oracle_lib.advance(r, params, dt, n_steps)
+    return {k: v for k, v in r.arrays()}, st
+
+
+VARIANTS = {
+    "default": dict(),
+    "no_friction": dict(use_neutral_friction=0),
+    "no_coriolis_damping": dict(use_coriolis=0, use_damping=1),
+    "log_ions": dict(use_improved_ion_advection=0),
+    "no_ion_advection": dict(use_ion_advection=0),
+    "beta1": dict(beta_limiter=1.0),
+    "given_coefficients": dict(compute_coefficients=0),
+    "no_nighttime_bcs": dict(use_nighttime_ion_bcs=0),
+}
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_step_matches_oracle(torch_cuda, oracle_lib, variant):
+    p = abi.default_params(**VARIANTS[variant])
+    m = synthetic.make_member(96, 50, seed=21)
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0)
+    out, st = gpu_advance(m, p, 2.0)
+    assert_state_close(out, ref, STATE)
+    np.testing.assert_array_equal(st, st_ref)
+
+
+def test_msis_lower_boundary(torch_cuda, oracle_lib):
+    p = abi.default_params(use_msis_bcs=1)
+    m = synthetic.make_member(64, 50, seed=22, with_lbc=True)
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0)
+    out, _ = gpu_advance(m, p, 2.0)
+    assert_state_close(out, ref, STATE)
+
+
+@pytest.mark.parametrize("n_alts", [8, 20, 75, 100, 128])
+def test_other_altitude_counts(torch_cuda, oracle_lib, n_alts):
+    p = abi.default_params()
+    m = synthetic.make_member(40, n_alts, seed=23 + n_alts)
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0)
+    out, _ = gpu_advance(m, p, 2.0)
+    assert_state_close(out, ref, STATE)
+
+
+@pytest.mark.parametrize("threads", [256, 320, 384])
+def test_launch_shapes_agree(torch_cuda, oracle_lib, threads):
+    p = abi.default_params()
+    m = synthetic.make_member(50, 50, seed=24)
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0)
+    out, _ = gpu_advance(m, p, 2.0, config=dict(threads=threads, ctas_per_sm=1))
+    assert_state_close(out, ref, STATE)
+
+
+def test_multistep_resident_matches_stepwise(torch_cuda, oracle_lib):
+    """steps_per_launch > 1 keeps columns in shared memory across steps."""
+    p = abi.default_params()
+    m = synthetic.make_member(64, 50, seed=25)
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0, n_steps=6)
+    out, _ = gpu_advance(m, p, 2.0, n_steps=6, config=dict(steps_per_launch=6))
+    assert_state_close(out, ref, STATE, rtol=1e-9)
+    out1, _ = gpu_advance(m, p, 2.0, n_steps=6, config=dict(steps_per_launch=1))
+    assert_state_close(out, out1, STATE, rtol=1e-12)
+
+
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_golden_fixtures(torch_cuda, path):
+    from tests.test_oracle import load_golden
+    p, m, out_ref, n_steps, dt, status = load_golden(path)
+    out, st = gpu_advance(m, p, dt, n_steps)
+    assert_state_close(out, out_ref, STATE, rtol=RTOL * 10 if n_steps > 1 else RTOL)
+    np.testing.assert_array_equal(st, status)
+
+
+def test_ragged_batch(torch_cuda, oracle_lib):
+    """Members of different nAlts and sizes advance in one launch."""
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    ms = [synthetic.make_member(n, na, seed=30 + i) for i, (n, na) in
+          enumerate([(37, 50), (20, 75), (13, 100), (5, 30)])]
+    refs = [ref_advance(oracle_lib, m, p, 2.0)[0] for m in ms]
+    ctx = V.VerticalContext(p)
+    dms = [V.device_member(m) for m in ms]
+    plan = V.Plan(ctx, dms)
+    plan.advance(2.0, 1)
+    plan.check()
+    for dm, ref in zip(dms, refs):
+        assert_state_close(dm.to_numpy(), ref, STATE)
+
+
+def test_neg_density_status(torch_cuda, oracle_lib):
+    p = abi.default_params()
+    m = synthetic.make_member(12, 50, seed=26)
+    m.ndensity_s[4, 20, 7] = -1.0
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0)
+    out, st = gpu_advance(m, p, 2.0)
+    assert st[7] & abi.ST_NEG_DENSITY and st_ref[7] & abi.ST_NEG_DENSITY
+    assert (st[np.arange(12) != 7] == 0).all()
+    assert_state_close(out, ref, synthetic.Member.STATE)
+
+
+def test_one_shot_raises_gitmstop(torch_cuda):
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(8, 50, seed=27)
+    m.ndensity_s[0, 5, 3] = 0.0
+    ctx = V.VerticalContext(p)
+    with pytest.raises(V.GitmStop):
+        V.advance_vertical_all(ctx, [V.device_member(m)], 2.0)
+
+
+def test_host_pointer_path_matches_device(torch_cuda, oracle_lib):
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(5000, 50, seed=28)
+    dev_out, _ = gpu_advance(m, p, 2.0)
+    h = m.copy()
+    ctx = V.VerticalContext(p)
+    V.advance_vertical_all_host(ctx, [h], 2.0)
+    for k in STATE:
+        np.testing.assert_array_equal(getattr(h, k), dev_out[k], err_msg=k)
+
+
+def test_modvertical_form(torch_cuda, oracle_lib):
+    import torch
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(48, 50, seed=29)
+    d = synthetic.to_modvertical(m, p)
+    ref = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+    oracle_lib.advance_1d(ref, p, 2.0)
+    td = {k: (torch.from_numpy(v).cuda() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+    ctx = V.VerticalContext(p)
+    V.advance_vertical_1d(ctx, td, 2.0)
+    got = {k: td[k].cpu().numpy() for k in ("log_rho", "temp", "vel_gd", "log_ns", "vert_vel")}
+    got["log_ins"] = td["log_ins"].cpu().numpy()[:9]
+    want = {k: ref[k] for k in ("log_rho", "temp", "vel_gd", "log_ns", "vert_vel")}
+    want["log_ins"] = ref["log_ins"][:9]
+    assert_state_close(got, want, list(got))
+
+
+def test_cfl_timestep(torch_cuda, oracle_lib):
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(300, 50, seed=31)
+    want = oracle_lib.cfl_dt(m, p, 0.75)
+    ctx = V.VerticalContext(p)
+    dm = V.device_member(m)
+    got = V.calc_timestep_vertical(ctx, [dm], cfl=0.75, dt=1e32, dt_end=1e32)
+    assert got == pytest.approx(want, rel=1e-14)
+    assert V.calc_timestep_vertical(ctx, [dm], cfl=0.75, dt=0.5) == 0.5
+
+
+def test_graph_capture_replays(torch_cuda, oracle_lib):
+    import torch
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(200, 50, seed=32)
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0, n_steps=3)
+    ctx = V.VerticalContext(p)
+    dm = V.device_member(m)
+    plan = V.Plan(ctx, [dm])
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            plan.advance(2.0, 1, stream=s)
+    torch.cuda.synchronize()
+    # capture does not execute: the state is still the input
+    np.testing.assert_array_equal(dm.tensors["rho"].cpu().numpy(), m.rho)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    plan.check()
+    assert_state_close(dm.to_numpy(), ref, STATE, rtol=1e-9)
+
+
+def test_autotune_leaves_state(torch_cuda):
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(3000, 50, seed=33)
+    ctx = V.VerticalContext(p)
+    dm = V.device_member(m)
+    plan = V.Plan(ctx, [dm])
+    cfg = plan.autotune(2.0, 2)
+    assert cfg.threads in (256, 320, 384)
+    np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
+    assert plan.status() == (0, 0)
