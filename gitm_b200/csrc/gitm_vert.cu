@@ -796,6 +796,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     }
     for (const ConstSpec& a : kInputs) {
       if (rc || !(d.*(a.field)) || !(b.*(a.field))) continue;
+      if (d.*(a.field) == b.*(a.field)) continue;  // shared grid: read from the host at plan creation
       if ((rc = h2d(const_cast<double*>(d.*(a.field)), b.*(a.field), rows_of(a.rows_per_cell, G)))) break;
     }
     if (rc) break;
