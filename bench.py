@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--deg", type=float, default=1.0, help="grid spacing in degrees")
     ap.add_argument("--n-alts", type=int, default=50)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--launch", default="", help="threads,steps_per_launch,ctas_per_sm (skips autotune)")
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--plain-steps", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -255,7 +256,10 @@ def run_ours(args):
         plan = V.Plan(ctx, [dm])
 
     # -- batched: autotuned launch shape, graph-captured steps
-    if not args.no_autotune:
+    if args.launch:
+        t, spl, cps = (int(x) for x in args.launch.split(","))
+        plan.set_config(threads=t, steps_per_launch=spl, ctas_per_sm=cps)
+    elif not args.no_autotune:
         plan.autotune(DT, min(args.steps, 8))
     cfg = plan.config
     plan.advance(DT, max(args.warmup, 1), stream=stream)
