@@ -11,7 +11,7 @@ import os
 from . import abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgitmvert.so")
+LIB_PATH = os.environ.get("GITM_VERT_LIB") or os.path.join(_HERE, "libgitmvert.so")
 _LIB = None
 
 # Every symbol include/gitm_vert.h declares, with (restype, argtypes).

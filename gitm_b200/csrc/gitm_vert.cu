@@ -93,6 +93,7 @@ static void fill_consts(Consts& k) {
   const double distinct[NS] = {0.774, 0.750, 0.749, 0.710, 0.718, 0.810};
   for (int s = 0; s < NS; ++s) {
     k.mass[s] = mass[s];
+    k.log_mass[s] = std::log(mass[s]);
     k.k_over_m[s] = KB / mass[s];
     k.inv_vib2[s] = 1.0 / (vib[s] - 2);
     k.one_minus_e[s] = 1.0 - distinct[s];
@@ -168,16 +169,32 @@ static void grid_coefs(int nA, const double* alt, const double* grav, const doub
 }
 
 // ------------------------------------------------------------------ kernels
+// Launch shapes built: threads per CTA -> CTAs per SM the registers allow and
+// where the RK accumulator lives.  The small CTAs keep it in shared memory so
+// that two or three CTAs share an SM and overlap each other's barriers.
+struct Shape { int threads, min_blocks; bool acc_smem; };
+static const Shape kShapes[] = {{128, 3, true}, {160, 2, true}, {192, 2, true},
+                                {256, 1, false}, {320, 1, false}, {384, 1, false}};
+static const int kThreadChoices[] = {128, 160, 192, 256, 320, 384};
+
+static bool acc_in_smem(int threads) {
+  for (const Shape& s : kShapes)
+    if (s.threads == threads) return s.acc_smem;
+  return false;
+}
+
 template <int IO>
 static const void* kernel_for(int threads) {
   switch (threads) {
-    case 256: return (const void*)vert_step_kernel<IO, 256>;
-    case 320: return (const void*)vert_step_kernel<IO, 320>;
-    case 384: return (const void*)vert_step_kernel<IO, 384>;
+    case 128: return (const void*)vert_step_kernel<IO, 128, 3, true>;
+    case 160: return (const void*)vert_step_kernel<IO, 160, 2, true>;
+    case 192: return (const void*)vert_step_kernel<IO, 192, 2, true>;
+    case 256: return (const void*)vert_step_kernel<IO, 256, 1, false>;
+    case 320: return (const void*)vert_step_kernel<IO, 320, 1, false>;
+    case 384: return (const void*)vert_step_kernel<IO, 384, 1, false>;
     default: return nullptr;
   }
 }
-static const int kThreadChoices[] = {256, 320, 384};
 
 // ------------------------------------------------------------------ API
 extern "C" {
@@ -275,23 +292,24 @@ static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int
   int nc = cfg.cols_per_cta > 0 ? cfg.cols_per_cta : cfg.threads / nA;
   nc = std::min(nc, cfg.threads / 32);  // one BC warp per column
   nc = std::min(nc, cfg.threads / nA);  // every interior cell has a thread
-  while (nc > 1 && smem_bytes(nA, nc) > ctx->max_smem) --nc;
+  while (nc > 1 && smem_bytes(nA, nc, acc_in_smem(cfg.threads)) > ctx->max_smem) --nc;
   return std::max(nc, 1);
 }
 
 static int build_tiles(GitmVertPlan* P) {
   GitmVertCtx* ctx = P->ctx;
   if (!kernel_for<0>(P->cfg.threads))
-    return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built (256, 320, 384)", P->cfg.threads);
+    return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built (128..384)", P->cfg.threads);
   P->tiles.clear();
   P->smem = 0;
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnBatch& b = P->host_members[m];
     const int nc = cols_per_cta(ctx, P->cfg, b.n_alts);
-    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc) > ctx->max_smem)
+    const bool as = acc_in_smem(P->cfg.threads);
+    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc, as) > ctx->max_smem)
       return set_err(ctx, GITM_ERR_ARG, "nAlts %d does not fit a CTA of %d threads", b.n_alts,
                      P->cfg.threads);
-    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc));
+    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc, as));
     for (int64_t c0 = 0; c0 < b.n_cols; c0 += nc) {
       Tile t;
       t.member = m;
@@ -588,7 +606,7 @@ extern "C" int gitm_vert_plan_autotune(GitmVertPlan* P, double dt, int n_steps, 
   std::vector<GitmLaunchConfig> cands;
   for (int t : kThreadChoices)
     for (int spl : {1, n_steps})
-      for (int cps : {0, 1, 2}) {
+      for (int cps : {0, 1, 2, 3}) {
         GitmLaunchConfig c{t, 0, spl, cps};
         cands.push_back(c);
       }

@@ -47,6 +47,7 @@ constexpr int NBC = 20;  // lower mesh coefs (cells 0,-1) x5, upper (nAlts+1,+2)
 // Earth constants (ModConstants.f90:11,15; ModEarth.f90:237-281,307-312).
 struct Consts {
   double mass[NS];
+  double log_mass[NS];
   double k_over_m[NS];
   double inv_vib2[NS];           // 1 / (Vibration - 2)
   double kc[NS][NS];             // 1e-2 k / (Mass_i Diff0_ij): friction coefficient

@@ -37,16 +37,20 @@ __device__ __forceinline__ int exp_index(int r, int q) {
 // ------------------------------------------------------------ smem layout
 struct Layout {
   int nAlts, G;
-  int X, XP, O, OP, LC, DL, TU, CM, GM, SC, stride;
+  int X, XP, O, OP, LC, DL, TU, CM, GM, SC, ACC, stride;
 };
 
-constexpr int NSC = 32;  // per-column scalars
+constexpr int NSC = 64;  // per-column scalars
 enum Scalar : int {
   SC_CENT = 0, SC_CORI = 1, SC_SZA = 2, SC_MLAT = 3, SC_MMM_M1 = 4, SC_MMM_0 = 5,
-  SC_PLASMA = 6, SC_HASLBC = 7, SC_LBC = 8  // 8..27: lbc[2][10]
+  SC_PLASMA = 6, SC_HASLBC = 7,
+  SC_LBC = 8,   // 8..27: lbc[2][10]
+  SC_BCC = 28,  // 28..47: mesh coefficients, lower cells 0, -1 then upper nA+1, nA+2
+  SC_DAF = 48,  // 48..53: dAlt_F at -1, 0, 1, nA, nA+1, nA+2
+  SC_EG = 54    // 54..58: Gravity + Centrifugal / InvR at -1, 0, nA, nA+1, nA+2
 };
 
-__host__ __device__ inline Layout make_layout(int nAlts) {
+__host__ __device__ inline Layout make_layout(int nAlts, bool acc_smem = false) {
   Layout L;
   L.nAlts = nAlts;
   L.G = nAlts + 4;
@@ -62,13 +66,14 @@ __host__ __device__ inline Layout make_layout(int nAlts) {
   L.CM = o; o += G;
   L.GM = o; o += G;
   L.SC = o; o += NSC;
+  L.ACC = o; o += acc_smem ? NF * nAlts : 0;  // RK accumulator when not in registers
   L.stride = o;
   return L;
 }
 
 // Bytes of dynamic shared memory a tile of nc columns needs.
-__host__ __device__ inline size_t smem_bytes(int nAlts, int nc) {
-  Layout L = make_layout(nAlts);
+__host__ __device__ inline size_t smem_bytes(int nAlts, int nc, bool acc_smem = false) {
+  Layout L = make_layout(nAlts, acc_smem);
   return size_t(L.stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
 }
 
@@ -133,216 +138,275 @@ __device__ __forceinline__ double lane_seq_sum(double v, int n) {
 }
 
 // ------------------------------------------------------------ boundaries
-// set_vertical_bcs (Earth), set_vertical_bcs.Earth.f90:8-652, for one column,
-// executed by one full warp.  IVel ghosts and the electron slot are not set:
-// nothing on the path reads them.
-__device__ void bc_column(const ColCtx& c, const GitmVertParams& prm, int lane, uint32_t* st) {
+// set_vertical_bcs (Earth), set_vertical_bcs.Earth.f90:8-652, for one column.
+// part 1 = lower boundary (cells -1, 0), part 2 = upper boundary (nAlts+1,
+// nAlts+2), part 3 = both; the two halves touch disjoint cells and can run on
+// different warps.  Executed by a full warp, lanes over species / ions.
+//
+// Where the reference goes through exp and back through log with a factor
+// that is exactly 1 (Temp(-1) = Temp(0) and Temp(nAlts+1:nAlts+2) =
+// Temp(nAlts) make the temperature ratios 1), the hydrostatic cells are
+// formed directly in log space: LogNS(-1) = LogNS(0) + dz/H, LogNS(nA+1) =
+// LogNS(nA) - dz/H.  IVel ghosts and the electron slot are not set: nothing
+// on the path reads them.
+__device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, int lane,
+                                          uint32_t* st, int part) {
   const int nA = c.L.nAlts;
-  const bool msis = prm.use_msis_bcs && c.sc(SC_HASLBC) != 0.0;
+  const int G = c.L.G;
+  double* X = c.col + c.L.X + 1;  // X[f*G + i]
+  const double* sc = c.col + c.L.SC;
   const bool improved = prm.use_improved_ion_advection != 0;
   const int s = lane;
+  auto x = [&](int f, int i) -> double& { return X[f * G + i]; };
 
-  // NS(0) and NS(nAlts) as exp(LogNS) on entry (line 93, before the MSIS
-  // values overwrite cell 0)
-  double nsb = 0.0, nst = 0.0;
-  if (s < NS) {
-    nsb = exp(c.x(F_LNS + s, 0));
-    nst = exp(c.x(F_LNS + s, nA));
-  }
-  __syncwarp();
-  // lines 112-148
-  if (msis) {
-    const double* t = &c.col[c.L.SC + SC_LBC];
-    if (s < NS) {
-      c.x(F_LNS + s, -1) = t[s];
-      c.x(F_LNS + s, 0) = t[10 + s];
-    } else if (s == 6) {
-      c.x(F_T, -1) = t[6];
-      c.x(F_T, 0) = t[16];
-    } else if (s == 7) {
-      c.x(F_LRHO, -1) = t[7];
-      c.x(F_LRHO, 0) = t[17];
-    } else if (s == 8) {
-      c.x(F_VE, -1) = t[8];
-      c.x(F_VE, 0) = t[18];
-    } else if (s == 9) {
-      c.x(F_VN, -1) = t[9];
-      c.x(F_VN, 0) = t[19];
-    }
-  } else {
-    if (s == 8) { c.x(F_VE, -1) = 0.0; c.x(F_VE, 0) = 0.0; }
-    if (s == 9) { c.x(F_VN, -1) = 0.0; c.x(F_VN, 0) = 0.0; }
-  }
-  if (s == 10) { c.x(F_VU, -1) = 0.0; c.x(F_VU, 0) = 0.0; }
-  if (s < NS) { c.x(F_W + s, -1) = 0.0; c.x(F_W + s, 0) = 0.0; }
-  __syncwarp();
-  // lines 192-196
-  if (s == 0) {
-    c.x(F_T, -1) = c.x(F_T, 0);
-    c.x(F_VE, -1) = c.x(F_VE, 0);
-    c.x(F_VN, -1) = c.x(F_VN, 0);
-    c.x(F_VU, -1) = c.x(F_VU, 0);
-  }
-  __syncwarp();
-  // lines 198-275: species at cell -1 (hydrostatic) / 0,-1 (photochemical)
-  if (s < NS) {
-    if (!photochemical(s)) {
-      double MeanGravity = -0.5 * (c.effg(-1) + c.effg(0));
-      double MeanTemp = 0.5 * (c.x(F_T, 0) + c.x(F_T, -1));
-      double MeanMass = 0.5 * (c.sc(SC_MMM_0) + c.sc(SC_MMM_M1));
-      double ish = MeanGravity * MeanMass / (MeanTemp * KB);
-      double ns = nsb * (c.x(F_T, 0) / c.x(F_T, -1)) * exp(ish * c.dAF(-1));
-      c.x(F_LNS + s, -1) = (s == 0) ? c.x(F_LNS + s, 0) : log(ns);
+  if (part & 1) {
+    const bool msis = prm.use_msis_bcs && sc[SC_HASLBC] != 0.0;
+    // LogNS(0) on entry: NS(0) of line 93 is formed before the MSIS values
+    // overwrite cell 0
+    const double l0 = (s < NS) ? x(F_LNS + s, 0) : 0.0;
+    __syncwarp();
+    // lines 112-148
+    if (msis) {
+      const double* t = sc + SC_LBC;
+      if (s < NS) {
+        x(F_LNS + s, -1) = t[s];
+        x(F_LNS + s, 0) = t[10 + s];
+      } else if (s == 6) {
+        x(F_T, -1) = t[6];
+        x(F_T, 0) = t[16];
+      } else if (s == 7) {
+        x(F_LRHO, -1) = t[7];
+        x(F_LRHO, 0) = t[17];
+      } else if (s == 8) {
+        x(F_VE, -1) = t[8];
+        x(F_VE, 0) = t[18];
+      } else if (s == 9) {
+        x(F_VN, -1) = t[9];
+        x(F_VN, 0) = t[19];
+      }
     } else {
+      if (s == 8) { x(F_VE, -1) = 0.0; x(F_VE, 0) = 0.0; }
+      if (s == 9) { x(F_VN, -1) = 0.0; x(F_VN, 0) = 0.0; }
+    }
+    if (s == 10) { x(F_VU, -1) = 0.0; x(F_VU, 0) = 0.0; }
+    if (s < NS) { x(F_W + s, -1) = 0.0; x(F_W + s, 0) = 0.0; }
+    __syncwarp();
+    // lines 192-196
+    if (s == 0) {
+      x(F_T, -1) = x(F_T, 0);
+      x(F_VE, -1) = x(F_VE, 0);
+      x(F_VN, -1) = x(F_VN, 0);
+      x(F_VU, -1) = x(F_VU, 0);
+    }
+    __syncwarp();
+    const double* bl = sc + SC_BCC;  // lower mesh coefficients, cell 0 then -1
+    if (s < NS) {
+      if (!photochemical(s)) {
+        // lines 205-222: hydrostatic cell -1 with the mean major mass
+        const double MeanGravity = -0.5 * (sc[SC_EG + 0] + sc[SC_EG + 1]);
+        const double MeanTemp = 0.5 * (x(F_T, 0) + x(F_T, -1));
+        const double MeanMass = 0.5 * (sc[SC_MMM_0] + sc[SC_MMM_M1]);
+        const double ish = MeanGravity * MeanMass / (MeanTemp * KB);
+        x(F_LNS + s, -1) = (s == 0) ? x(F_LNS + s, 0) : l0 + ish * sc[SC_DAF + 0];
+      } else {
+        // lines 226-272: 3rd-order extrapolation with a gradient limit
+        #pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int i = -k;
+          const double* C = bl + 5 * k;
+          const double d = x(F_LNS + s, i + 1) * C[0] + x(F_LNS + s, i + 2) * C[1] +
+                           x(F_LNS + s, i + 3) * C[2] + x(F_LNS + s, i + 4) * C[3] +
+                           x(F_LNS + s, i + 5) * C[4];
+          const double up = x(F_LNS + s, i + 1);
+          double v = up - sc[SC_DAF + 2 + i] * d;  // dAlt_F(i+1)
+          if (d <= 0.0) v = up;
+          if (s == 4 && v < up - 0.333) v = up - 0.333;
+          x(F_LNS + s, i) = v;
+        }
+      }
+      // vertical winds (lines 334-344)
+      #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const int i = -k;
-        double d = c.x(F_LNS + s, i + 1) * c.bcc(k * 5 + 0) + c.x(F_LNS + s, i + 2) * c.bcc(k * 5 + 1) +
-                   c.x(F_LNS + s, i + 3) * c.bcc(k * 5 + 2) + c.x(F_LNS + s, i + 4) * c.bcc(k * 5 + 3) +
-                   c.x(F_LNS + s, i + 5) * c.bcc(k * 5 + 4);
-        double up = c.x(F_LNS + s, i + 1);
-        double v = up - c.dAF(i + 1) * d;
-        if (d <= 0.0) v = up;
-        if (s == 4 && v < up - 0.333) v = up - 0.333;
-        c.x(F_LNS + s, i) = v;
+        const double* C = bl + 5 * k;
+        const double d = x(F_W + s, i + 1) * C[0] + x(F_W + s, i + 2) * C[1] +
+                         x(F_W + s, i + 3) * C[2] + x(F_W + s, i + 4) * C[3] +
+                         x(F_W + s, i + 5) * C[4];
+        x(F_W + s, i) = x(F_W + s, i + 1) - sc[SC_DAF + 2 + i] * d;
       }
     }
-  }
-  // ions float at the lower boundary (lines 304-310)
-  if (s < NI) {
-    c.ion(s, 0) = c.ion(s, 1);
-    c.ion(s, -1) = c.ion(s, 0);
-  }
-  // vertical winds, 3rd-order extrapolation (lines 334-344)
-  if (s < NS) {
-    for (int k = 0; k < 2; ++k) {
-      const int i = -k;
-      double d = c.x(F_W + s, i + 1) * c.bcc(k * 5 + 0) + c.x(F_W + s, i + 2) * c.bcc(k * 5 + 1) +
-                 c.x(F_W + s, i + 3) * c.bcc(k * 5 + 2) + c.x(F_W + s, i + 4) * c.bcc(k * 5 + 3) +
-                 c.x(F_W + s, i + 5) * c.bcc(k * 5 + 4);
-      c.x(F_W + s, i) = c.x(F_W + s, i + 1) - c.dAF(i + 1) * d;
+    // ions float at the lower boundary (lines 304-310)
+    if (s < NI) {
+      const double v = c.ion(s, 1);
+      c.ion(s, 0) = v;
+      c.ion(s, -1) = v;
     }
-  }
-  __syncwarp();
-  // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1
-  for (int k = 0; k < 2; ++k) {
-    const int i = -k;
-    double ns = 0.0, term = 0.0;
-    if (s < NS) {
-      ns = exp(c.x(F_LNS + s, i));
-      term = c_k.mass[s] * ns;
+    __syncwarp();
+    // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1
+    {
+      double m0 = 0.0, m1 = 0.0, t0 = 0.0, t1 = 0.0;
+      if (s < NS) {
+        m0 = c_k.mass[s] * exp(x(F_LNS + s, 0));
+        m1 = c_k.mass[s] * exp(x(F_LNS + s, -1));
+        t0 = m0 * x(F_W + s, 0);
+        t1 = m1 * x(F_W + s, -1);
+      }
+      const double r0 = lane_seq_sum(m0, NS), r1 = lane_seq_sum(m1, NS);
+      const double v0 = lane_seq_sum(t0, NS), v1 = lane_seq_sum(t1, NS);
+      if (s == 0) {
+        x(F_LRHO, 0) = log(r0);
+        x(F_VU, 0) = v0 / r0;
+      } else if (s == 1) {
+        x(F_LRHO, -1) = log(r1);
+        x(F_VU, -1) = v1 / r1;
+      }
     }
-    const double SumRho = lane_seq_sum(term, NS);
-    const double lr = log(SumRho);
-    const double er = exp(lr);
-    double t2 = 0.0;
-    if (s < NS) t2 = ns * c_k.mass[s] * c.x(F_W + s, i) / er;
-    const double vu = lane_seq_sum(t2, NS);
-    if (s == 0) {
-      c.x(F_LRHO, i) = lr;
-      c.x(F_VU, i) = vu;
+    // lines 364-376
+    if (msis && (s == 8 || s == 9)) {
+      const int f = (s == 8) ? F_VE : F_VN;
+      const double* C = bl + 5;
+      const double d = x(f, 0) * C[0] + x(f, 1) * C[1] + x(f, 2) * C[2] + x(f, 3) * C[3] + x(f, 4) * C[4];
+      x(f, -1) = x(f, 0) - sc[SC_DAF + 1] * d;
     }
-  }
-  // lines 364-376
-  if (msis && (s == 8 || s == 9)) {
-    const int f = (s == 8) ? F_VE : F_VN;
-    const int i = -1;
-    double d = c.x(f, i + 1) * c.bcc(5) + c.x(f, i + 2) * c.bcc(6) + c.x(f, i + 3) * c.bcc(7) +
-               c.x(f, i + 4) * c.bcc(8) + c.x(f, i + 5) * c.bcc(9);
-    c.x(f, i) = c.x(f, i + 1) - c.dAF(i + 1) * d;
-  }
-  __syncwarp();
-  // lines 382-395
-  if (s < NS && photochemical(s) && c.x(F_W + s, 1) > 0.0) {
-    c.x(F_W + s, 0) = -1.0 * c.x(F_W + s, 1);
-    c.x(F_W + s, -1) = -1.0 * c.x(F_W + s, 1);
+    __syncwarp();
+    // lines 382-395
+    if (s < NS && photochemical(s) && x(F_W + s, 1) > 0.0) {
+      x(F_W + s, 0) = -1.0 * x(F_W + s, 1);
+      x(F_W + s, -1) = -1.0 * x(F_W + s, 1);
+    }
   }
 
-  // ---- top, lines 420-463
-  if (s == 8) { c.x(F_VE, nA + 1) = c.x(F_VE, nA); c.x(F_VE, nA + 2) = c.x(F_VE, nA); }
-  if (s == 9) { c.x(F_VN, nA + 1) = c.x(F_VN, nA); c.x(F_VN, nA + 2) = c.x(F_VN, nA); }
-  if (s < NS) {
-    double wn = c.x(F_W + s, nA);
-    double w1 = wn, w2 = wn;
-    if (photochemical(s) && wn < 0.0) {
-      w1 = -wn;
-      w2 = -c.x(F_W + s, nA - 1);
+  if (part & 2) {
+    // lines 420-463
+    if (s == 8) { x(F_VE, nA + 1) = x(F_VE, nA); x(F_VE, nA + 2) = x(F_VE, nA); }
+    if (s == 9) { x(F_VN, nA + 1) = x(F_VN, nA); x(F_VN, nA + 2) = x(F_VN, nA); }
+    if (s < NS) {
+      const double wn = x(F_W + s, nA);
+      double w1 = wn, w2 = wn;
+      if (photochemical(s) && wn < 0.0) {
+        w1 = -wn;
+        w2 = -x(F_W + s, nA - 1);
+      }
+      x(F_W + s, nA + 1) = w1;
+      x(F_W + s, nA + 2) = w2;
+      // lines 471-486: hydrostatic neutrals, Temp(nA+1:nA+2) = Temp(nA)
+      const double T = x(F_T, nA);
+      const double ish1 = (-0.5 * (sc[SC_EG + 3] + sc[SC_EG + 2])) * c_k.mass[s] / (0.5 * (T + T) * KB);
+      const double ish2 = (-0.5 * (sc[SC_EG + 4] + sc[SC_EG + 3])) * c_k.mass[s] / (0.5 * (T + T) * KB);
+      const double l1 = x(F_LNS + s, nA) - ish1 * sc[SC_DAF + 4];
+      x(F_LNS + s, nA + 1) = l1;
+      x(F_LNS + s, nA + 2) = l1 - ish2 * sc[SC_DAF + 5];
     }
-    c.x(F_W + s, nA + 1) = w1;
-    c.x(F_W + s, nA + 2) = w2;
-  }
-  if (s == 10) {
-    double v = c.x(F_VU, nA);
-    double w = (v < 0.0) ? -v : v;
-    c.x(F_VU, nA + 1) = w;
-    c.x(F_VU, nA + 2) = w;
-  }
-  if (s == 11) {
-    c.x(F_T, nA + 1) = c.x(F_T, nA);
-    c.x(F_T, nA + 2) = c.x(F_T, nA);
-  }
-  __syncwarp();
-  // lines 471-486: hydrostatic neutrals
-  if (s < NS) {
-    double ns = nst;
-    for (int i = nA + 1; i <= nA + 2; ++i) {
-      double MeanGravity = -0.5 * (c.effg(i) + c.effg(i - 1));
-      double MeanTemp = 0.5 * (c.x(F_T, i - 1) + c.x(F_T, i));
-      double ish = MeanGravity * c_k.mass[s] / (MeanTemp * KB);
-      ns = ns * (c.x(F_T, i - 1) / c.x(F_T, i)) * exp(-ish * c.dAF(i));
-      c.x(F_LNS + s, i) = log(ns);
+    if (s == 10) {
+      const double v = x(F_VU, nA);
+      const double w = (v < 0.0) ? -v : v;
+      x(F_VU, nA + 1) = w;
+      x(F_VU, nA + 2) = w;
     }
-  }
-  // lines 497-501: TEC of the first ion
-  double tp = 0.0;
-  for (int i = 1 + lane; i <= nA; i += 32) {
-    double v = c.ion(0, i);
-    tp += c.dAF(i) * (improved ? v : exp(v));
-  }
-  for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
-  const double tec = tp / 1e16;
-  const bool hold = (tec < prm.min_tec) && (c.sc(SC_PLASMA) != 0.0);
-  // lines 503-596: ions at the top
-  if (s < NI) {
-    for (int k = 0; k < 2; ++k) {
-      const int iAlt = nA + 1 + k;
-      double n[6];
-      if (improved) {
-        // check_for_negative_densities, lines 608-649
-        double mn = c.ion(s, iAlt - 5);
-        for (int q = iAlt - 4; q <= iAlt; ++q) mn = fmin(mn, c.ion(s, q));
-        if (mn < 0.0) {
-          if (c.ion(s, iAlt - 6) < 0.0) atomicOr(st, GITM_ST_NEG_ION_TOP);
-          for (int q = iAlt - 5; q <= iAlt - 1; ++q) {
-            if (c.ion(s, q) < 0.0) {
-              if (c.ion(s, q - 1) > 0.0 && c.ion(s, q + 1) > 0.0)
-                c.ion(s, q) = (c.ion(s, q - 1) + c.ion(s, q + 1)) / 2.0;
-              else
-                c.ion(s, q) = c.ion(s, q - 1) * 0.95;
-            }
-          }
-          if (c.ion(s, iAlt) < 0.0) c.ion(s, iAlt) = c.ion(s, iAlt - 1) * 0.95;
+    if (s == 11) {
+      x(F_T, nA + 1) = x(F_T, nA);
+      x(F_T, nA + 2) = x(F_T, nA);
+    }
+    // lines 497-501: TEC of the first ion
+    double tp = 0.0;
+    for (int i = 1 + lane; i <= nA; i += 32) {
+      const double v = c.ion(0, i);
+      tp += c.dAF(i) * (improved ? v : exp(v));
+    }
+    for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
+    const bool hold = (tp / 1e16 < prm.min_tec) && (sc[SC_PLASMA] != 0.0);
+    const double* bu = sc + SC_BCC + 10;  // upper mesh coefficients, nA+1 then nA+2
+    // check_for_negative_densities (lines 608-649) can only act when a value
+    // in nAlts-5 .. nAlts+2 is negative
+    bool neg = false;
+    if (improved && s < NI)
+      for (int q = nA - 5; q <= nA + 2; ++q) neg = neg || (c.ion(s, q) < 0.0);
+    const bool anyneg = __any_sync(0xffffffffu, neg);
+    if (!improved) {
+      if (s < NI && !hold) {
+        #pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int iAlt = nA + 1 + k;
+          const double* C = bu + 5 * k;
+          double dn = C[0] * c.ion(s, iAlt - 1) + C[1] * c.ion(s, iAlt - 2) + C[2] * c.ion(s, iAlt - 3) +
+                      C[3] * c.ion(s, iAlt - 4) + C[4] * c.ion(s, iAlt - 5);
+          const double lim = -(0.001 * c.ion(s, iAlt) / sc[SC_DAF + 3]);
+          if (dn > lim) dn = lim;
+          c.ion(s, iAlt) = c.ion(s, iAlt - 1) + dn * sc[SC_DAF + 4 + k];
         }
-        for (int j = 0; j < 6; ++j) n[j] = log(c.ion(s, iAlt - j));
-      } else {
-        for (int j = 0; j < 6; ++j) n[j] = c.ion(s, iAlt - j);
       }
-      double dn = c.bcc(10 + 5 * k + 0) * n[1] + c.bcc(10 + 5 * k + 1) * n[2] +
-                  c.bcc(10 + 5 * k + 2) * n[3] + c.bcc(10 + 5 * k + 3) * n[4] +
-                  c.bcc(10 + 5 * k + 4) * n[5];
-      if (!hold) {
-        const double lim = -(0.001 * n[0] / c.dAF(nA));
+    } else if (anyneg) {
+      // the reference's order, one ion per lane
+      if (s < NI) {
+        #pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int iAlt = nA + 1 + k;
+          double mn = c.ion(s, iAlt - 5);
+          for (int q = iAlt - 4; q <= iAlt; ++q) mn = fmin(mn, c.ion(s, q));
+          if (mn < 0.0) {
+            if (c.ion(s, iAlt - 6) < 0.0) atomicOr(st, GITM_ST_NEG_ION_TOP);
+            for (int q = iAlt - 5; q <= iAlt - 1; ++q) {
+              if (c.ion(s, q) < 0.0) {
+                if (c.ion(s, q - 1) > 0.0 && c.ion(s, q + 1) > 0.0)
+                  c.ion(s, q) = (c.ion(s, q - 1) + c.ion(s, q + 1)) / 2.0;
+                else
+                  c.ion(s, q) = c.ion(s, q - 1) * 0.95;
+              }
+            }
+            if (c.ion(s, iAlt) < 0.0) c.ion(s, iAlt) = c.ion(s, iAlt - 1) * 0.95;
+          }
+          double n[6];
+          #pragma unroll
+          for (int j = 0; j < 6; ++j) n[j] = log(c.ion(s, iAlt - j));
+          if (!hold) {
+            const double* C = bu + 5 * k;
+            double dn = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
+            const double lim = -(0.001 * n[0] / sc[SC_DAF + 3]);
+            if (dn > lim) dn = lim;
+            c.ion(s, iAlt) = exp(n[1] + dn * sc[SC_DAF + 4 + k]);
+          }
+        }
+      }
+    } else if (!hold) {
+      // no negative value: the logs of the 9 ions x 6 cells are independent,
+      // so the warp takes them two per lane; the second cell reuses four.
+      double* lg = c.col + c.L.DL;  // scratch: the slopes are dead during the BCs
+      for (int q = lane; q < NI * 6; q += 32) {
+        const int si = q / 6, j = q - si * 6;
+        lg[q] = log(c.ion(si, nA + 1 - j));
+      }
+      __syncwarp();
+      double n1 = 0.0;
+      if (s < NI) {
+        const double* n = lg + s * 6;
+        const double* C = bu;
+        double dn = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
+        const double lim = -(0.001 * n[0] / sc[SC_DAF + 3]);
         if (dn > lim) dn = lim;
-        const double n0 = n[1] + dn * c.dAF(iAlt);
-        c.ion(s, iAlt) = improved ? exp(n0) : n0;
+        const double v = exp(n[1] + dn * sc[SC_DAF + 4]);
+        c.ion(s, nA + 1) = v;
+        // cell nAlts+2: logs of its own ghost and of the value just set
+        const double g0 = log(c.ion(s, nA + 2));
+        n1 = log(v);
+        const double* D = bu + 5;
+        double dn2 = D[0] * n1 + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
+        const double lim2 = -(0.001 * g0 / sc[SC_DAF + 3]);
+        if (dn2 > lim2) dn2 = lim2;
+        c.ion(s, nA + 2) = exp(n1 + dn2 * sc[SC_DAF + 5]);
       }
     }
-  }
-  __syncwarp();
-  // lines 598-604
-  for (int i = nA + 1; i <= nA + 2; ++i) {
-    double term = (s < NS) ? c_k.mass[s] * exp(c.x(F_LNS + s, i)) : 0.0;
-    double SumRho = lane_seq_sum(term, NS);
-    if (s == 0) c.x(F_LRHO, i) = log(SumRho);
+    __syncwarp();
+    // lines 598-604
+    {
+      double m1 = 0.0, m2 = 0.0;
+      if (s < NS) {
+        m1 = c_k.mass[s] * exp(x(F_LNS + s, nA + 1));
+        m2 = c_k.mass[s] * exp(x(F_LNS + s, nA + 2));
+      }
+      const double r1 = lane_seq_sum(m1, NS), r2 = lane_seq_sum(m2, NS);
+      if (s == 0) x(F_LRHO, nA + 1) = log(r1);
+      if (s == 1) x(F_LRHO, nA + 2) = log(r2);
+    }
   }
   __syncwarp();
 }
@@ -363,8 +427,8 @@ constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
 
 // IO = 0: GITM arrays (advance_vertical gather/scatter);
 // IO = 1: ModVertical arrays (advance_vertical_1d_* arguments).
-template <int IO, int NT>
-__global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
+template <int IO, int NT, int MINB, bool ACC_SMEM>
+__global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -377,7 +441,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
     const DevMember& M = kp.members[tile.member];
     const int nA = M.b.n_alts;
     const int nc = tile.nc;
-    const Layout L = make_layout(nA);
+    const Layout L = make_layout(nA, ACC_SMEM);
     const int G = L.G;
     const int64_t ncols = M.b.n_cols;
     uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(L.stride) * nc);  // [nc] status
@@ -398,6 +462,16 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
     };
     auto gidx = [&](int f, int g, int cl) -> int64_t {
       return (int64_t(f) * G + g) * ncols + tile.c0 + cl;
+    };
+    // set_vertical_bcs for every column of the tile: the lower and upper
+    // halves of a column go to different warps when there are enough
+    auto boundaries = [&]() {
+      constexpr int nw = NT / 32;
+      if (2 * nc <= nw) {
+        if (wid < 2 * nc) bc_column(ctx(wid >> 1), prm, lane, &sst[wid >> 1], 1 + (wid & 1));
+      } else {
+        for (int cl = wid; cl < nc; cl += nw) bc_column(ctx(cl), prm, lane, &sst[cl], 3);
+      }
     };
 
     if (tid < nc) {
@@ -435,17 +509,30 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
       c.sc(SC_PLASMA) = plasma ? 1.0 : 0.0;
       const double* lbc = (IO == 0) ? M.b.lbc : M.mv.lbc;
       c.sc(SC_HASLBC) = lbc ? 1.0 : 0.0;
+      // boundary constants of this column's grid
+      #pragma unroll
+      for (int j = 0; j < 20; ++j) c.sc(SC_BCC + j) = c.bcc(j);
+      const int dcell[6] = {-1, 0, 1, nA, nA + 1, nA + 2};
+      #pragma unroll
+      for (int j = 0; j < 6; ++j) c.sc(SC_DAF + j) = c.dAF(dcell[j]);
+      const int ecell[5] = {-1, 0, nA, nA + 1, nA + 2};
+      #pragma unroll
+      for (int j = 0; j < 5; ++j) c.sc(SC_EG + j) = c.g(GC_GRAV, ecell[j]) + cent * c.g(GC_R, ecell[j]);
       if (lbc)
+        #pragma unroll
         for (int k = 0; k < 2 * GITM_LBC_NVALUES; ++k)
           c.sc(SC_LBC + k) = lbc[int64_t(k) * ncols + cc];
     }
+    // columns vary fastest across threads so that a warp reads whole
+    // row segments of the native layout
     for (int w = tid; w < nc * G; w += NT) {
-      const int cl = w / G, g = w - cl * G, i = g - 1;
+      const int g = w / nc, cl = w - g * nc, i = g - 1;
       ColCtx c = ctx(cl);
       if (IO == 0) {
         const GitmColumnBatch& b = M.b;
         double nd[NS], ww[NS];
         double mn = 1.0;
+        #pragma unroll
         for (int s = 0; s < NS; ++s) {
           nd[s] = b.ndensity_s[gidx(s, g, cl)];
           ww[s] = b.vert_vel[gidx(s, g, cl)];
@@ -458,18 +545,22 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           // calc_pressure.f90:17-21,56-83; calc_rates.Earth.f90:34-50;
           // calc_timestep.f90:114-118
           double N = 0.0;
+          #pragma unroll
           for (int s = 0; s < NS; ++s) N = N + nd[s];
           double gg = 0.0;
+          #pragma unroll
           for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
           gamma = gg * 2.0 / N + 1;
           double m = 0.0;
           const double rn = 1.0 / (N + 1.0);
+          #pragma unroll
           for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
           if (m == 0) m = c_k.mass[0];
           mmm = m;
           tu = m * (1.0 / KB);
           if (g >= 1 && g <= nA + 2) {
             double mx = fabs(ww[0]);
+            #pragma unroll
             for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(ww[s]));
             cmx = mx + sqrt(gamma * temperature);
           }
@@ -490,6 +581,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         c.gm(i) = gamma;
         if (i == -1) c.sc(SC_MMM_M1) = mmm;
         if (i == 0) c.sc(SC_MMM_0) = mmm;
+        #pragma unroll
         for (int s = 0; s < NS; ++s) {
           c.x(F_LNS + s, i) = log(nd[s]);
           c.x(F_W + s, i) = ww[s];
@@ -500,6 +592,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         c.x(F_VU, i) = b.velocity[gidx(2, g, cl)];
         c.x(F_LRHO, i) = log(b.rho[gidx(0, g, cl)]);
         const bool pc = in_pcells(i, nA);
+        #pragma unroll
         for (int s = 0; s < NI; ++s) {
           if (s >= NADV && !pc) continue;
           const double v = b.idensity_s[gidx(s, g, cl)];
@@ -507,6 +600,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         }
       } else {
         const GitmModVerticalBatch& b = M.mv;
+        #pragma unroll
         for (int s = 0; s < NS; ++s) {
           c.x(F_LNS + s, i) = b.log_ns[gidx(s, g, cl)];
           c.x(F_W + s, i) = b.vert_vel[gidx(s, g, cl)];
@@ -517,6 +611,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         c.x(F_VU, i) = b.vel_gd[gidx(2, g, cl)];
         c.x(F_LRHO, i) = b.log_rho[gidx(0, g, cl)];
         const bool pc = in_pcells(i, nA);
+        #pragma unroll
         for (int s = 0; s < NI; ++s) {
           if (s >= NADV && !pc) continue;
           c.ion(s, i) = b.log_ins[gidx(s, g, cl)];
@@ -528,11 +623,11 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         if (i == 0) c.sc(SC_MMM_0) = b.mean_major_mass[gidx(0, g, cl)];
       }
     }
-    __syncthreads();
+    __syncthreads();  // @phase 0
 
     // per-item constants for the step
     double eddy = 0.0, ivup = 0.0;
-    double acc[NF];
+    double acc[ACC_SMEM ? 1 : NF];
 
     for (int step = 0; step < kp.n_steps; ++step) {
       if (item) {
@@ -545,8 +640,8 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         }
       }
       // ---------------------------------------------------- first BC pass
-      if (wid < nc) bc_column(ctx(wid), prm, lane, &sst[wid]);
-      __syncthreads();
+      boundaries();
+      __syncthreads();  // @phase 1
       // Orig = state (vertical_solver_rusanov.f90:95-100)
       for (int w = tid; w < nc * (NF * G + NPAS * NPC); w += NT) {
         const int per = NF * G + NPAS * NPC;
@@ -564,17 +659,14 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
         // -------------------------------------------------- phase A
         // LogConS on every cell (vertical_solver_rusanov.f90:506-509) and the
         // limited slopes of the 18 swept fields on cells 0..nAlts+1
-        // (calc_facevalues_alts_rusanov, :745-772).
-        double ns[NS], rho = 1.0;
+        // (calc_facevalues_alts_rusanov, :745-772).  LogConS = log(m n_s / Rho)
+        // is formed as log(m_s) + LogNS - LogRho, without the exp/log pair.
         if (item) {
           ColCtx c = ctx(my_cl);
           const int i = my_i;
-          rho = exp(c.x(F_LRHO, i));
-          const double ir = 1.0 / rho;
-          for (int s = 0; s < NS; ++s) {
-            ns[s] = exp(c.x(F_LNS + s, i));
-            c.lc(s, i) = log(c_k.mass[s] * ns[s] * ir);
-          }
+          const double lr = c.x(F_LRHO, i);
+#pragma unroll
+          for (int s = 0; s < NS; ++s) c.lc(s, i) = c_k.log_mass[s] + c.x(F_LNS + s, i) - lr;
           const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
 #pragma unroll 2
           for (int f = 0; f < NSTENCIL; ++f) {
@@ -591,8 +683,9 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           ColCtx c = ctx(cl);
           if (u < 4) {
             const int i = (u < 2) ? u - 1 : nA + u - 1;  // -1, 0, nA+1, nA+2
-            const double ir = 1.0 / exp(c.x(F_LRHO, i));
-            for (int s = 0; s < NS; ++s) c.lc(s, i) = log(c_k.mass[s] * exp(c.x(F_LNS + s, i)) * ir);
+            const double lr = c.x(F_LRHO, i);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) c.lc(s, i) = c_k.log_mass[s] + c.x(F_LNS + s, i) - lr;
           } else {
             const int i = (u == 4) ? 0 : nA + 1;
             const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
@@ -602,13 +695,18 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             }
           }
         }
-        __syncthreads();
+        __syncthreads();  // @phase 2
 
         // -------------------------------------------------- phase B
         double kv[NF];
         if (item) {
           ColCtx c = ctx(my_cl);
           const int i = my_i;
+          // NS = exp(LogNS), 1 / Rho (vertical_solver_rusanov.f90:466-467)
+          double ns[NS];
+          const double rho = exp(-c.x(F_LRHO, i));  // holds 1 / Rho
+#pragma unroll
+          for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
           const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
           const double idc = c.g(GC_IDC, i);
           const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
@@ -637,6 +735,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           const double divv = gU + 2 * VU * invr;
           kv[F_T] = (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T;
           // ions 1..nIonsAdvect (:557-568)
+          #pragma unroll
           for (int s = 0; s < NADV; ++s) {
             double gI, dI;
             sweep(F_I + s, gI, dI);
@@ -644,13 +743,14 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             kv[F_I + s] = (I - dt * (ivup * gI) + dt * dI) - I;
           }
           // species continuity and momentum (:548-617)
-          const double tau = prm.use_damping
-                                 ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
-                                 : prm.vert_tau;
+          const double itau = 1.0 / (prm.use_damping
+                                         ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
+                                         : prm.vert_tau);
           const double hz = (VN * VN + VE * VE) * invr;
           const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
           double wv[NS];
           double sumrho = 0.0;
+#pragma unroll
           for (int s = 0; s < NS; ++s) {
             double gL, dL, gW, dW;
             sweep(F_LNS + s, gL, dL);
@@ -661,9 +761,9 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             kv[F_LNS + s] = nl - Ls;
             sumrho = sumrho + c_k.mass[s] * exp(nl);
             const double km = c_k.k_over_m[s];
-            double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws / tau;
+            double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
             w = w + cor;
-            w = w - dt * (prm.thermal_diff_coef[s] * KB * gT) / c_k.mass[s];
+            w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
             wv[s] = w;
           }
           kv[F_LRHO] = log(sumrho) - c.x(F_LRHO, i);
@@ -672,6 +772,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             double glc[NS];
             const double m0 = c.g(GC_M0 + 0, i), m1 = c.g(GC_M0 + 1, i), m2 = c.g(GC_M0 + 2, i),
                          m3 = c.g(GC_M0 + 3, i), m4 = c.g(GC_M0 + 4, i);
+            #pragma unroll
             for (int s = 0; s < NS; ++s)
               glc[s] = m0 * c.lc(s, i - 2) + m1 * c.lc(s, i - 1) + m2 * c.lc(s, i) +
                        m3 * c.lc(s, i + 1) + m4 * c.lc(s, i + 2);
@@ -712,11 +813,13 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
               for (int q = r + 1; q < NS; ++q) sum -= a[r][q] * wv[q];
               wv[r] = sum * a[r][r];
             }
+            #pragma unroll
             for (int s = 0; s < NS; ++s) wv[s] = wv[s] + (-eddy * glc[s]);
           }
           // clamp and bulk vertical wind (:643-658)
-          const double ir = 1.0 / rho;
+          const double ir = rho;
           double vu = 0.0;
+          #pragma unroll
           for (int s = 0; s < NS; ++s) {
             double w = fmax(-prm.max_vertical_velocity, wv[s]);
             w = fmin(prm.max_vertical_velocity, w);
@@ -725,7 +828,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           }
           kv[F_VU] = vu - VU;
         }
-        __syncthreads();
+        __syncthreads();  // @phase 3
 
         // -------------------------------------------------- RK update
         // vertical_solver_rusanov.f90:120-163,190-232,261-303,330-366
@@ -734,11 +837,18 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           const int i = my_i;
 #pragma unroll
           for (int f = 0; f < NF; ++f) {
-            if (k == 0) acc[f] = kv[f];
-            else if (k < 3) acc[f] = acc[f] + 2.0 * kv[f];
-            else acc[f] = acc[f] + kv[f];
+            double a;
+            if constexpr (ACC_SMEM) {
+              double& as = c.col[L.ACC + f * nA + i - 1];
+              a = (k == 0) ? kv[f] : (k < 3) ? as + 2.0 * kv[f] : as + kv[f];
+              as = a;
+            } else {
+              const int fa = ACC_SMEM ? 0 : f;
+              a = (k == 0) ? kv[f] : (k < 3) ? acc[fa] + 2.0 * kv[f] : acc[fa] + kv[f];
+              acc[fa] = a;
+            }
             const double o = c.o(f, i);
-            c.x(f, i) = (k < 2) ? o + 0.5 * kv[f] : (k == 2) ? o + kv[f] : o + (1.0 / 6.0) * acc[f];
+            c.x(f, i) = (k < 2) ? o + 0.5 * kv[f] : (k == 2) ? o + kv[f] : o + (1.0 / 6.0) * a;
           }
         }
         // ghost cells and passive ions return to Orig (their K is zero)
@@ -754,25 +864,26 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             col[L.XP + r - NF * 4] = col[L.OP + r - NF * 4];
           }
         }
-        __syncthreads();
+        __syncthreads();  // @phase 4
         if (k < 3) {
-          if (wid < nc) bc_column(ctx(wid), prm, lane, &sst[wid]);
-          __syncthreads();
+          boundaries();
+          __syncthreads();  // @phase 1
         }
       }
       // final set_vertical_bcs (:368-369)
-      if (wid < nc) bc_column(ctx(wid), prm, lane, &sst[wid]);
-      __syncthreads();
+      boundaries();
+      __syncthreads();  // @phase 1
 
       // ---------------------------------------------------- store / reload
       const bool last = (step == kp.n_steps - 1);
       for (int w = tid; w < nc * G; w += NT) {
-        const int cl = w / G, g = w - cl * G, i = g - 1;
+        const int g = w / nc, cl = w - g * nc, i = g - 1;
         ColCtx c = ctx(cl);
         const bool store = last && sfrozen[cl] == 0u;
         if (IO == 1) {
           if (!store) continue;
           const GitmModVerticalBatch& b = M.mv;
+          #pragma unroll
           for (int s = 0; s < NS; ++s) {
             b.log_ns[gidx(s, g, cl)] = c.x(F_LNS + s, i);
             b.vert_vel[gidx(s, g, cl)] = c.x(F_W + s, i);
@@ -783,16 +894,18 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           b.vel_gd[gidx(2, g, cl)] = c.x(F_VU, i);
           b.log_rho[gidx(0, g, cl)] = c.x(F_LRHO, i);
           const bool pc = in_pcells(i, nA);
+          #pragma unroll
           for (int s = 0; s < NI; ++s)
             if (s < NADV || pc) b.log_ins[gidx(s, g, cl)] = c.ion(s, i);
           continue;
         }
         // scatter, advance_vertical.f90:163-217
         const GitmColumnBatch& b = M.b;
-        const double rho = exp(c.x(F_LRHO, i));
+        const double rho = store ? exp(c.x(F_LRHO, i)) : 1.0;
         const double temperature = c.x(F_T, i) / c.tu(i);
         double nd[NS], N = 0.0;
         bool finite = isfinite(rho) && isfinite(temperature);
+        #pragma unroll
         for (int s = 0; s < NS; ++s) {
           nd[s] = exp(c.x(F_LNS + s, i));
           N = N + nd[s];
@@ -807,6 +920,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           b.velocity[gidx(1, g, cl)] = c.x(F_VN, i);
           b.velocity[gidx(2, g, cl)] = c.x(F_VU, i);
           b.temperature[gidx(0, g, cl)] = temperature;
+          #pragma unroll
           for (int s = 0; s < NS; ++s) {
             if (b.log_ns) b.log_ns[gidx(s, g, cl)] = c.x(F_LNS + s, i);
             b.vert_vel[gidx(s, g, cl)] = c.x(F_W + s, i);
@@ -815,6 +929,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           if (b.ndensity) b.ndensity[gidx(0, g, cl)] = N;
           if (prm.use_ion_advection) {
             double e = 0.0;
+            #pragma unroll
             for (int s = 0; s < NI; ++s) {
               double v;
               if (s < NADV || pc) {
@@ -836,14 +951,17 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           // the next step's gather from the values just formed
           double gamma = c.gm(i), mmm = 0.0, tu = c.tu(i), cmx = c.cm(i);
           bool bad = false;
+          #pragma unroll
           for (int s = 0; s < NS; ++s) bad = bad || !(nd[s] > 0.0);
           if (bad) atomicOr(&sst[cl], GITM_ST_NEG_DENSITY);
           if (prm.compute_coefficients) {
             double gg = 0.0;
+            #pragma unroll
             for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
             gamma = gg * 2.0 / N + 1;
             double m = 0.0;
             const double rn = 1.0 / (N + 1.0);
+            #pragma unroll
             for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
             if (m == 0) m = c_k.mass[0];
             mmm = m;
@@ -851,6 +969,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             cmx = 0.0;
             if (g >= 1 && g <= nA + 2) {
               double mx = fabs(c.x(F_W, i));
+              #pragma unroll
               for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(c.x(F_W + s, i)));
               cmx = mx + sqrt(gamma * temperature);
             }
@@ -866,10 +985,12 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
             if (i == -1) c.sc(SC_MMM_M1) = mmm;
             if (i == 0) c.sc(SC_MMM_0) = mmm;
           }
-          for (int s = 0; s < NS; ++s) c.x(F_LNS + s, i) = log(nd[s]);
+                    // LogNS = log(NDensityS) and LogRho = log(Rho) of the next gather
+          // (advance_vertical.f90:105,114) give back the values in X up to a
+          // rounding of exp/log, so X keeps them
           c.x(F_T, i) = temperature * tu;
-          c.x(F_LRHO, i) = log(rho);
           if (prm.use_ion_advection) {
+            #pragma unroll
             for (int s = 0; s < NI; ++s) {
               if (!(s < NADV || pc)) continue;
               double v = c.ion(s, i);
@@ -880,7 +1001,7 @@ __global__ void __launch_bounds__(NT, 1) vert_step_kernel(const KParams kp) {
           }
         }
       }
-      __syncthreads();
+      __syncthreads();  // @phase 5
     }
 
     if (tid < nc) {

@@ -228,6 +228,6 @@ def test_autotune_leaves_state(torch_cuda):
     dm = V.device_member(m)
     plan = V.Plan(ctx, [dm])
     cfg = plan.autotune(2.0, 2)
-    assert cfg.threads in (256, 320, 384)
+    assert cfg.threads in (128, 160, 192, 256, 320, 384)
     np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
     assert plan.status() == (0, 0)
