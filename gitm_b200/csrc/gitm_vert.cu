@@ -53,6 +53,9 @@ struct GitmVertPlan {
   std::vector<Tile> tiles;
   Tile* d_tiles = nullptr;
   size_t smem = 0;
+  int grid = 0;                 // CTAs per launch for the current cfg
+  double* d_scratch = nullptr;  // RK accumulators of persistent CTAs
+  size_t scratch_doubles = 0;
   int max_nalts = 0, min_nalts = 1 << 30;
 };
 
@@ -170,16 +173,17 @@ static void grid_coefs(int nA, const double* alt, const double* grav, const doub
 
 // ------------------------------------------------------------------ kernels
 // Launch shapes built: threads per CTA -> CTAs per SM the registers allow and
-// where the RK accumulator lives.  The small CTAs keep it in shared memory so
-// that two or three CTAs share an SM and overlap each other's barriers.
-struct Shape { int threads, min_blocks; bool acc_smem; };
+// where the RK accumulator lives.  The small CTAs keep it in a per-CTA slot
+// of global scratch (L2-resident under their persistent grid) so that two or
+// three CTAs share an SM and overlap each other's barrier phases.
+struct Shape { int threads, min_blocks; bool acc_global; };
 static const Shape kShapes[] = {{128, 3, true}, {160, 2, true}, {192, 2, true},
                                 {256, 1, false}, {320, 1, false}, {384, 1, false}};
 static const int kThreadChoices[] = {128, 160, 192, 256, 320, 384};
 
-static bool acc_in_smem(int threads) {
+static bool acc_global(int threads) {
   for (const Shape& s : kShapes)
-    if (s.threads == threads) return s.acc_smem;
+    if (s.threads == threads) return s.acc_global;
   return false;
 }
 
@@ -292,7 +296,7 @@ static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int
   int nc = cfg.cols_per_cta > 0 ? cfg.cols_per_cta : cfg.threads / nA;
   nc = std::min(nc, cfg.threads / 32);  // one BC warp per column
   nc = std::min(nc, cfg.threads / nA);  // every interior cell has a thread
-  while (nc > 1 && smem_bytes(nA, nc, acc_in_smem(cfg.threads)) > ctx->max_smem) --nc;
+  while (nc > 1 && smem_bytes(nA, nc) > ctx->max_smem) --nc;
   return std::max(nc, 1);
 }
 
@@ -305,11 +309,10 @@ static int build_tiles(GitmVertPlan* P) {
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnBatch& b = P->host_members[m];
     const int nc = cols_per_cta(ctx, P->cfg, b.n_alts);
-    const bool as = acc_in_smem(P->cfg.threads);
-    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc, as) > ctx->max_smem)
+    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc) > ctx->max_smem)
       return set_err(ctx, GITM_ERR_ARG, "nAlts %d does not fit a CTA of %d threads", b.n_alts,
                      P->cfg.threads);
-    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc, as));
+    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc));
     for (int64_t c0 = 0; c0 < b.n_cols; c0 += nc) {
       Tile t;
       t.member = m;
@@ -324,6 +327,32 @@ static int build_tiles(GitmVertPlan* P) {
     CUDA_TRY(ctx, cudaMalloc(&P->d_tiles, P->tiles.size() * sizeof(Tile)));
     CUDA_TRY(ctx, cudaMemcpy(P->d_tiles, P->tiles.data(), P->tiles.size() * sizeof(Tile),
                              cudaMemcpyHostToDevice));
+  }
+  // grid: one CTA per tile, or a persistent grid of ctas_per_sm x SMs; shapes
+  // that keep the accumulator in scratch always run persistent (one slot per CTA)
+  const int T = P->cfg.threads;
+  int grid = int(P->tiles.size());
+  int per_sm = P->cfg.ctas_per_sm;
+  if (acc_global(T) && per_sm <= 0) {
+    const void* fn = (P->io == 0) ? kernel_for<0>(T) : kernel_for<1>(T);
+    CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->smem));
+    per_sm = std::max(per_sm, 1);
+  }
+  if (per_sm > 0) grid = std::min(grid, per_sm * ctx->num_sms);
+  P->grid = std::max(grid, 1);
+  if (acc_global(T)) {
+    // at least three slots: the host-pointer path splits them over 3 streams
+    const size_t need = size_t(std::max(P->grid, 3)) * NF * T;
+    if (need > P->scratch_doubles) {
+      cudaFree(P->d_scratch);
+      P->d_scratch = nullptr;
+      P->scratch_doubles = 0;
+      if (cudaMalloc(&P->d_scratch, need * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, GITM_ERR_NOMEM, "cannot allocate %zu bytes of step scratch", need * sizeof(double));
+      }
+      P->scratch_doubles = need;
+    }
   }
   return GITM_OK;
 }
@@ -395,6 +424,7 @@ static int plan_common(GitmVertPlan* P, const double* const* alt, const double* 
 
 static void plan_free(GitmVertPlan* P) {
   if (!P) return;
+  cudaFree(P->d_scratch);
   cudaFree(P->d_members);
   cudaFree(P->d_grid);
   cudaFree(P->d_status);
@@ -499,14 +529,14 @@ static int launch_steps(GitmVertPlan* P, double dt, int n_steps, cudaStream_t st
   const int spl = std::max(1, P->cfg.steps_per_launch);
   const void* fn = (P->io == 0) ? kernel_for<0>(P->cfg.threads) : kernel_for<1>(P->cfg.threads);
   if (!fn) return set_err(ctx, GITM_ERR_ARG, "no kernel for %d threads", P->cfg.threads);
-  int grid = int(P->tiles.size());
-  if (P->cfg.ctas_per_sm > 0) grid = std::min(grid, P->cfg.ctas_per_sm * ctx->num_sms);
+  const int grid = P->grid;
   KParams kp;
   kp.members = P->d_members;
   kp.tiles = P->d_tiles;
   kp.n_tiles = int(P->tiles.size());
   kp.dt = dt;
   kp.status = P->d_status;
+  kp.scratch = P->d_scratch;
   kp.prm = ctx->params;
   for (int done = 0; done < n_steps; done += spl) {
     kp.n_steps = std::min(spl, n_steps - done);
@@ -825,11 +855,17 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     kp.n_tiles = t0[j + 1] - t0[j];
     kp.dt = dt;
     kp.status = P->d_status;
+    kp.scratch = P->d_scratch;
     kp.prm = prm;
+    // chunks run on three streams at once: each gets a third of the
+    // persistent grid's scratch slots
+    const int third = std::max(1, P->grid / 3);
+    if (P->d_scratch) kp.scratch = P->d_scratch + size_t(j % 3) * third * NF * P->cfg.threads;
+    const int cgrid = P->d_scratch ? std::min(kp.n_tiles, third) : kp.n_tiles;
     for (int done = 0; done < n_steps && kp.n_tiles > 0; done += spl) {
       kp.n_steps = std::min(spl, n_steps - done);
       void* args[] = {&kp};
-      cudaError_t e = cudaLaunchKernel(fn, dim3(kp.n_tiles), dim3(P->cfg.threads), args, P->smem, st);
+      cudaError_t e = cudaLaunchKernel(fn, dim3(cgrid), dim3(P->cfg.threads), args, P->smem, st);
       if (e != cudaSuccess) { rc = set_err(ctx, GITM_ERR_CUDA, "launch: %s", cudaGetErrorString(e)); break; }
     }
     for (const ArraySpec& a : kArrays) {

@@ -37,7 +37,7 @@ __device__ __forceinline__ int exp_index(int r, int q) {
 // ------------------------------------------------------------ smem layout
 struct Layout {
   int nAlts, G;
-  int X, XP, O, OP, LC, DL, TU, CM, GM, SC, ACC, stride;
+  int X0, XP0, X1, XP1, O, OP, DL, TU, CM, GM, SC, stride;
 };
 
 constexpr int NSC = 64;  // per-column scalars
@@ -50,30 +50,33 @@ enum Scalar : int {
   SC_EG = 54    // 54..58: Gravity + Centrifugal / InvR at -1, 0, nA, nA+1, nA+2
 };
 
-__host__ __device__ inline Layout make_layout(int nAlts, bool acc_smem = false) {
+// Per-column shared-memory slot (doubles): the stage state twice (a stage
+// reads one buffer and writes the next), Orig, the limited slopes, the
+// per-cell coefficients and the column scalars.
+__host__ __device__ inline Layout make_layout(int nAlts) {
   Layout L;
   L.nAlts = nAlts;
   L.G = nAlts + 4;
   const int G = L.G;
   int o = 0;
-  L.X = o;  o += NF * G;
-  L.XP = o; o += NPAS * NPC;
-  L.O = o;  o += NF * G;
-  L.OP = o; o += NPAS * NPC;
-  L.LC = o; o += NS * G;
-  L.DL = o; o += NSTENCIL * (nAlts + 2);
-  L.TU = o; o += G;
-  L.CM = o; o += G;
-  L.GM = o; o += G;
-  L.SC = o; o += NSC;
-  L.ACC = o; o += acc_smem ? NF * nAlts : 0;  // RK accumulator when not in registers
+  L.X0 = o;  o += NF * G;
+  L.XP0 = o; o += NPAS * NPC;
+  L.X1 = o;  o += NF * G;
+  L.XP1 = o; o += NPAS * NPC;
+  L.O = o;   o += NF * G;
+  L.OP = o;  o += NPAS * NPC;
+  L.DL = o;  o += NSTENCIL * (nAlts + 2);
+  L.TU = o;  o += G;
+  L.CM = o;  o += G;
+  L.GM = o;  o += G;
+  L.SC = o;  o += NSC;
   L.stride = o;
   return L;
 }
 
 // Bytes of dynamic shared memory a tile of nc columns needs.
-__host__ __device__ inline size_t smem_bytes(int nAlts, int nc, bool acc_smem = false) {
-  Layout L = make_layout(nAlts, acc_smem);
+__host__ __device__ inline size_t smem_bytes(int nAlts, int nc) {
+  Layout L = make_layout(nAlts);
   return size_t(L.stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
 }
 
@@ -102,19 +105,20 @@ struct ColCtx {
   Layout L;
   const double* gridc;
   int gcols;
-  int gc;  // grid column (0 when the member shares one grid)
+  int gc;   // grid column (0 when the member shares one grid)
+  int xo;   // offset of the current stage buffer (X0 or X1)
+  int xpo;  // offset of its passive-ion cells (XP0 or XP1)
 
-  __device__ __forceinline__ double& x(int f, int i) const { return col[L.X + f * L.G + i + 1]; }
+  __device__ __forceinline__ double& x(int f, int i) const { return col[xo + f * L.G + i + 1]; }
   __device__ __forceinline__ double& o(int f, int i) const { return col[L.O + f * L.G + i + 1]; }
-  __device__ __forceinline__ double& lc(int s, int i) const { return col[L.LC + s * L.G + i + 1]; }
   __device__ __forceinline__ double& dl(int f, int c) const { return col[L.DL + f * (L.nAlts + 2) + c]; }
   __device__ __forceinline__ double& sc(int k) const { return col[L.SC + k]; }
   __device__ __forceinline__ double& cm(int i) const { return col[L.CM + i + 1]; }
   __device__ __forceinline__ double& tu(int i) const { return col[L.TU + i + 1]; }
   __device__ __forceinline__ double& gm(int i) const { return col[L.GM + i + 1]; }
   __device__ __forceinline__ double& ion(int s, int i) const {
-    return (s < NADV) ? col[L.X + (F_I + s) * L.G + i + 1]
-                      : col[L.XP + (s - NADV) * NPC + pcell(i, L.nAlts)];
+    return (s < NADV) ? col[xo + (F_I + s) * L.G + i + 1]
+                      : col[xpo + (s - NADV) * NPC + pcell(i, L.nAlts)];
   }
   // grid coefficient k at Fortran cell i
   __device__ __forceinline__ double g(int k, int i) const {
@@ -124,9 +128,6 @@ struct ColCtx {
     return __ldg(gridc + (size_t(NGC) * L.G + j) * gcols + gc);
   }
   __device__ __forceinline__ double dAF(int i) const { return g(GC_DALTF, i); }
-  __device__ __forceinline__ double effg(int i) const {
-    return g(GC_GRAV, i) + sc(SC_CENT) * g(GC_R, i);  // Gravity + Centrifugal / InvR
-  }
 };
 
 // Sequential sum over lanes 0..n-1 of v (same order as a Fortran DO loop
@@ -153,7 +154,7 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
                                           uint32_t* st, int part) {
   const int nA = c.L.nAlts;
   const int G = c.L.G;
-  double* X = c.col + c.L.X + 1;  // X[f*G + i]
+  double* X = c.col + c.xo + 1;  // X[f*G + i]
   const double* sc = c.col + c.L.SC;
   const bool improved = prm.use_improved_ion_advection != 0;
   const int s = lane;
@@ -418,7 +419,8 @@ struct KParams {
   int n_tiles;
   int n_steps;
   double dt;
-  uint32_t* status;  // one word per column (member col_offset + column)
+  uint32_t* status;   // one word per column (member col_offset + column)
+  double* scratch;    // RK accumulators, NF * NT doubles per CTA (ACC_GLOBAL)
   GitmVertParams prm;
 };
 
@@ -427,7 +429,10 @@ constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
 
 // IO = 0: GITM arrays (advance_vertical gather/scatter);
 // IO = 1: ModVertical arrays (advance_vertical_1d_* arguments).
-template <int IO, int NT, int MINB, bool ACC_SMEM>
+// ACC_GLOBAL: the RK accumulator of each item lives in a per-CTA slot of
+// kp.scratch (coalesced, L2-resident under a persistent grid) instead of
+// registers, which lets small CTAs share an SM.
+template <int IO, int NT, int MINB, bool ACC_GLOBAL>
 __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
@@ -435,13 +440,14 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   const int wid = tid >> 5;
   const GitmVertParams& prm = kp.prm;
   const double dt = kp.dt;
+  double* accg = ACC_GLOBAL ? kp.scratch + size_t(blockIdx.x) * NF * NT + tid : nullptr;
 
   for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
     const Tile tile = kp.tiles[tix];
     const DevMember& M = kp.members[tile.member];
     const int nA = M.b.n_alts;
     const int nc = tile.nc;
-    const Layout L = make_layout(nA, ACC_SMEM);
+    const Layout L = make_layout(nA);
     const int G = L.G;
     const int64_t ncols = M.b.n_cols;
     uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(L.stride) * nc);  // [nc] status
@@ -450,6 +456,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
     const bool item = tid < nitems;
     const int my_cl = item ? tid / nA : 0;
     const int my_i = item ? tid % nA + 1 : 1;
+    int cur = 0;  // stage buffer holding the current state
 
     auto ctx = [&](int cl) {
       ColCtx c;
@@ -458,6 +465,8 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
       c.gridc = M.gridc;
       c.gcols = M.gcols;
       c.gc = (M.gcols == 1) ? 0 : int(tile.c0 + cl);
+      c.xo = cur ? L.X1 : L.X0;
+      c.xpo = cur ? L.XP1 : L.XP0;
       return c;
     };
     auto gidx = [&](int f, int g, int cl) -> int64_t {
@@ -509,22 +518,18 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
       c.sc(SC_PLASMA) = plasma ? 1.0 : 0.0;
       const double* lbc = (IO == 0) ? M.b.lbc : M.mv.lbc;
       c.sc(SC_HASLBC) = lbc ? 1.0 : 0.0;
-      // boundary constants of this column's grid
-      #pragma unroll
-      for (int j = 0; j < 20; ++j) c.sc(SC_BCC + j) = c.bcc(j);
-      const int dcell[6] = {-1, 0, 1, nA, nA + 1, nA + 2};
-      #pragma unroll
-      for (int j = 0; j < 6; ++j) c.sc(SC_DAF + j) = c.dAF(dcell[j]);
-      const int ecell[5] = {-1, 0, nA, nA + 1, nA + 2};
-      #pragma unroll
-      for (int j = 0; j < 5; ++j) c.sc(SC_EG + j) = c.g(GC_GRAV, ecell[j]) + cent * c.g(GC_R, ecell[j]);
       if (lbc)
-        #pragma unroll
         for (int k = 0; k < 2 * GITM_LBC_NVALUES; ++k)
           c.sc(SC_LBC + k) = lbc[int64_t(k) * ncols + cc];
+      // boundary constants of this column's grid
+      for (int j = 0; j < 20; ++j) c.sc(SC_BCC + j) = c.bcc(j);
+      const int dcell[6] = {-1, 0, 1, nA, nA + 1, nA + 2};
+      for (int j = 0; j < 6; ++j) c.sc(SC_DAF + j) = c.dAF(dcell[j]);
+      const int ecell[5] = {-1, 0, nA, nA + 1, nA + 2};
+      for (int j = 0; j < 5; ++j) c.sc(SC_EG + j) = c.g(GC_GRAV, ecell[j]) + cent * c.g(GC_R, ecell[j]);
     }
-    // columns vary fastest across threads so that a warp reads whole
-    // row segments of the native layout
+    // columns vary fastest across threads so that a warp reads whole row
+    // segments of the native layout
     for (int w = tid; w < nc * G; w += NT) {
       const int g = w / nc, cl = w - g * nc, i = g - 1;
       ColCtx c = ctx(cl);
@@ -532,7 +537,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         const GitmColumnBatch& b = M.b;
         double nd[NS], ww[NS];
         double mn = 1.0;
-        #pragma unroll
+#pragma unroll
         for (int s = 0; s < NS; ++s) {
           nd[s] = b.ndensity_s[gidx(s, g, cl)];
           ww[s] = b.vert_vel[gidx(s, g, cl)];
@@ -545,22 +550,22 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           // calc_pressure.f90:17-21,56-83; calc_rates.Earth.f90:34-50;
           // calc_timestep.f90:114-118
           double N = 0.0;
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) N = N + nd[s];
           double gg = 0.0;
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
           gamma = gg * 2.0 / N + 1;
           double m = 0.0;
           const double rn = 1.0 / (N + 1.0);
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
           if (m == 0) m = c_k.mass[0];
           mmm = m;
           tu = m * (1.0 / KB);
           if (g >= 1 && g <= nA + 2) {
             double mx = fabs(ww[0]);
-            #pragma unroll
+#pragma unroll
             for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(ww[s]));
             cmx = mx + sqrt(gamma * temperature);
           }
@@ -581,7 +586,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         c.gm(i) = gamma;
         if (i == -1) c.sc(SC_MMM_M1) = mmm;
         if (i == 0) c.sc(SC_MMM_0) = mmm;
-        #pragma unroll
+#pragma unroll
         for (int s = 0; s < NS; ++s) {
           c.x(F_LNS + s, i) = log(nd[s]);
           c.x(F_W + s, i) = ww[s];
@@ -592,7 +597,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         c.x(F_VU, i) = b.velocity[gidx(2, g, cl)];
         c.x(F_LRHO, i) = log(b.rho[gidx(0, g, cl)]);
         const bool pc = in_pcells(i, nA);
-        #pragma unroll
+#pragma unroll
         for (int s = 0; s < NI; ++s) {
           if (s >= NADV && !pc) continue;
           const double v = b.idensity_s[gidx(s, g, cl)];
@@ -600,7 +605,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         }
       } else {
         const GitmModVerticalBatch& b = M.mv;
-        #pragma unroll
+#pragma unroll
         for (int s = 0; s < NS; ++s) {
           c.x(F_LNS + s, i) = b.log_ns[gidx(s, g, cl)];
           c.x(F_W + s, i) = b.vert_vel[gidx(s, g, cl)];
@@ -611,7 +616,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         c.x(F_VU, i) = b.vel_gd[gidx(2, g, cl)];
         c.x(F_LRHO, i) = b.log_rho[gidx(0, g, cl)];
         const bool pc = in_pcells(i, nA);
-        #pragma unroll
+#pragma unroll
         for (int s = 0; s < NI; ++s) {
           if (s >= NADV && !pc) continue;
           c.ion(s, i) = b.log_ins[gidx(s, g, cl)];
@@ -627,7 +632,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
 
     // per-item constants for the step
     double eddy = 0.0, ivup = 0.0;
-    double acc[ACC_SMEM ? 1 : NF];
+    double accr[ACC_GLOBAL ? 1 : NF];
 
     for (int step = 0; step < kp.n_steps; ++step) {
       if (item) {
@@ -642,78 +647,78 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
       // ---------------------------------------------------- first BC pass
       boundaries();
       __syncthreads();  // @phase 1
-      // Orig = state (vertical_solver_rusanov.f90:95-100)
-      for (int w = tid; w < nc * (NF * G + NPAS * NPC); w += NT) {
+      // Orig = state (vertical_solver_rusanov.f90:95-100); read first in
+      // phase B, after the barrier that ends phase A
+      {
+        const int xo = cur ? L.X1 : L.X0;  // X and its passive cells are contiguous
         const int per = NF * G + NPAS * NPC;
-        const int cl = w / per, r = w - cl * per;
-        double* col = sm + size_t(L.stride) * cl;
-        if (r < NF * G)
-          col[L.O + r] = col[L.X + r];
-        else
-          col[L.OP + r - NF * G] = col[L.XP + r - NF * G];
+        for (int w = tid; w < nc * per; w += NT) {
+          const int cl = w / per, r = w - cl * per;
+          double* col = sm + size_t(L.stride) * cl;
+          col[L.O + r] = col[xo + r];
+        }
       }
-      // no barrier needed here: the stage below reads X only until its
-      // first barrier, and Orig is first read after it
 
       for (int k = 0; k < 4; ++k) {
         // -------------------------------------------------- phase A
-        // LogConS on every cell (vertical_solver_rusanov.f90:506-509) and the
         // limited slopes of the 18 swept fields on cells 0..nAlts+1
-        // (calc_facevalues_alts_rusanov, :745-772).  LogConS = log(m n_s / Rho)
-        // is formed as log(m_s) + LogNS - LogRho, without the exp/log pair.
+        // (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772)
         if (item) {
           ColCtx c = ctx(my_cl);
           const int i = my_i;
-          const double lr = c.x(F_LRHO, i);
-#pragma unroll
-          for (int s = 0; s < NS; ++s) c.lc(s, i) = c_k.log_mass[s] + c.x(F_LNS + s, i) - lr;
           const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
-#pragma unroll 2
+#pragma unroll 3
           for (int f = 0; f < NSTENCIL; ++f) {
-            const double* v = &c.col[L.X + f * G + 1];
+            const double* v = &c.col[c.xo + f * G + 1];
             const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
             const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
             c.dl(f, i) = limiter_mc(up, dn, prm.beta_limiter);
           }
         }
-        // extra units: LogConS of the 4 ghost cells and the two end slopes
-        for (int q = tid - nitems; q < nc * 6; q += NT) {
+        // the two end slopes of each column (:764-772)
+        for (int q = tid - nitems; q < nc * 2; q += NT) {
           if (q < 0) continue;
-          const int cl = q / 6, u = q - cl * 6;
+          const int cl = q >> 1;
           ColCtx c = ctx(cl);
-          if (u < 4) {
-            const int i = (u < 2) ? u - 1 : nA + u - 1;  // -1, 0, nA+1, nA+2
-            const double lr = c.x(F_LRHO, i);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) c.lc(s, i) = c_k.log_mass[s] + c.x(F_LNS + s, i) - lr;
-          } else {
-            const int i = (u == 4) ? 0 : nA + 1;
-            const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
-            for (int f = 0; f < NSTENCIL; ++f) {
-              const double* v = &c.col[L.X + f * G + 1];
-              c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, prm.beta_limiter);
-            }
+          const int i = (q & 1) ? nA + 1 : 0;
+          const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+          for (int f = 0; f < NSTENCIL; ++f) {
+            const double* v = &c.col[c.xo + f * G + 1];
+            c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, prm.beta_limiter);
           }
         }
         __syncthreads();  // @phase 2
 
         // -------------------------------------------------- phase B
-        double kv[NF];
+        // advance_vertical_1stage (:387-686) at the item's cell; the stage
+        // result goes straight into the other buffer as Orig + c_k K_k
+        // (vertical_solver_rusanov.f90:120-163,190-232,261-303,350-366)
+        const int nxo = cur ? L.X0 : L.X1;
         if (item) {
           ColCtx c = ctx(my_cl);
           const int i = my_i;
-          // NS = exp(LogNS), 1 / Rho (vertical_solver_rusanov.f90:466-467)
-          double ns[NS];
-          const double rho = exp(-c.x(F_LRHO, i));  // holds 1 / Rho
-#pragma unroll
-          for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
+          double* xn = c.col + nxo + 1;  // next buffer, xn[f*G + i]
+          auto emit = [&](int f, double kval) {
+            double a;
+            if constexpr (ACC_GLOBAL) {
+              double& ag = accg[size_t(f) * NT];
+              a = (k == 0) ? kval : (k < 3) ? ag + 2.0 * kval : ag + kval;
+              ag = a;
+            } else {
+              const int fa = ACC_GLOBAL ? 0 : f;
+              a = (k == 0) ? kval : (k < 3) ? accr[fa] + 2.0 * kval : accr[fa] + kval;
+              accr[fa] = a;
+            }
+            const double o = c.o(f, i);
+            xn[f * G + i] = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
+          };
           const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
           const double idc = c.g(GC_IDC, i);
           const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
           const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
           // calc_rusanov_alts_rusanov (:694-718) at cell i
           auto sweep = [&](int f, double& grad, double& diff) {
-            const double* v = &c.col[L.X + f * G + 1];
+            const double* v = &c.col[c.xo + f * G + 1];
             const double* d = &c.col[L.DL + f * (nA + 2)];
             const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
             const double R0 = v[i] - 0.5 * d[i] * dF0;
@@ -724,23 +729,26 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           };
           const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
           const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
-          double gT, dT, gE, dE, gN, dN, gU, dU;
+          double gT, dT;
           sweep(F_T, gT, dT);
-          sweep(F_VE, gE, dE);
-          sweep(F_VN, gN, dN);
-          sweep(F_VU, gU, dU);
-          // :660-680
-          kv[F_VE] = (VE - dt * VU * gE + dt * dE) - VE;
-          kv[F_VN] = (VN - dt * VU * gN + dt * dN) - VN;
-          const double divv = gU + 2 * VU * invr;
-          kv[F_T] = (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T;
+          {
+            double gE, dE, gN, dN, gU, dU;
+            sweep(F_VE, gE, dE);
+            sweep(F_VN, gN, dN);
+            sweep(F_VU, gU, dU);
+            // :660-680
+            emit(F_VE, (VE - dt * VU * gE + dt * dE) - VE);
+            emit(F_VN, (VN - dt * VU * gN + dt * dN) - VN);
+            const double divv = gU + 2 * VU * invr;
+            emit(F_T, (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T);
+          }
           // ions 1..nIonsAdvect (:557-568)
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NADV; ++s) {
             double gI, dI;
             sweep(F_I + s, gI, dI);
             const double I = c.x(F_I + s, i);
-            kv[F_I + s] = (I - dt * (ivup * gI) + dt * dI) - I;
+            emit(F_I + s, (I - dt * (ivup * gI) + dt * dI) - I);
           }
           // species continuity and momentum (:548-617)
           const double itau = 1.0 / (prm.use_damping
@@ -758,7 +766,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
             const double divw = gW + 2 * Ws * invr;
             const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
-            kv[F_LNS + s] = nl - Ls;
+            emit(F_LNS + s, nl - Ls);
             sumrho = sumrho + c_k.mass[s] * exp(nl);
             const double km = c_k.k_over_m[s];
             double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
@@ -766,16 +774,33 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
             wv[s] = w;
           }
-          kv[F_LRHO] = log(sumrho) - c.x(F_LRHO, i);
+          const double LR = c.x(F_LRHO, i);
+          emit(F_LRHO, log(sumrho) - LR);
+          // NS = exp(LogNS), 1 / Rho (:466-467)
+          double ns[NS];
+#pragma unroll
+          for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
+          const double ir = exp(-LR);
           // calc_neutral_friction (calc_neutral_friction.f90:47-106)
           if (prm.use_neutral_friction) {
+            // GradLogConS (:506-543), LogConS = log(m_s) + LogNS - LogRho
             double glc[NS];
-            const double m0 = c.g(GC_M0 + 0, i), m1 = c.g(GC_M0 + 1, i), m2 = c.g(GC_M0 + 2, i),
-                         m3 = c.g(GC_M0 + 3, i), m4 = c.g(GC_M0 + 4, i);
-            #pragma unroll
-            for (int s = 0; s < NS; ++s)
-              glc[s] = m0 * c.lc(s, i - 2) + m1 * c.lc(s, i - 1) + m2 * c.lc(s, i) +
-                       m3 * c.lc(s, i + 1) + m4 * c.lc(s, i + 2);
+            {
+              double mc[5], lr5[5];
+#pragma unroll
+              for (int q = 0; q < 5; ++q) {
+                mc[q] = c.g(GC_M0 + q, i);
+                lr5[q] = c.x(F_LRHO, i - 2 + q);
+              }
+#pragma unroll
+              for (int s = 0; s < NS; ++s) {
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+                  acc += mc[q] * (c_k.log_mass[s] + c.x(F_LNS + s, i - 2 + q) - lr5[q]);
+                glc[s] = acc;
+              }
+            }
             const double lt = log(T);
             double pw[NS];
 #pragma unroll
@@ -813,66 +838,43 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
               for (int q = r + 1; q < NS; ++q) sum -= a[r][q] * wv[q];
               wv[r] = sum * a[r][r];
             }
-            #pragma unroll
+#pragma unroll
             for (int s = 0; s < NS; ++s) wv[s] = wv[s] + (-eddy * glc[s]);
           }
           // clamp and bulk vertical wind (:643-658)
-          const double ir = rho;
           double vu = 0.0;
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) {
             double w = fmax(-prm.max_vertical_velocity, wv[s]);
             w = fmin(prm.max_vertical_velocity, w);
-            kv[F_W + s] = w - c.x(F_W + s, i);
+            emit(F_W + s, w - c.x(F_W + s, i));
             vu = vu + w * (c_k.mass[s] * ns[s] * ir);
           }
-          kv[F_VU] = vu - VU;
+          emit(F_VU, vu - VU);
         }
-        __syncthreads();  // @phase 3
-
-        // -------------------------------------------------- RK update
-        // vertical_solver_rusanov.f90:120-163,190-232,261-303,330-366
-        if (item) {
-          ColCtx c = ctx(my_cl);
-          const int i = my_i;
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            double a;
-            if constexpr (ACC_SMEM) {
-              double& as = c.col[L.ACC + f * nA + i - 1];
-              a = (k == 0) ? kv[f] : (k < 3) ? as + 2.0 * kv[f] : as + kv[f];
-              as = a;
-            } else {
-              const int fa = ACC_SMEM ? 0 : f;
-              a = (k == 0) ? kv[f] : (k < 3) ? acc[fa] + 2.0 * kv[f] : acc[fa] + kv[f];
-              acc[fa] = a;
-            }
-            const double o = c.o(f, i);
-            c.x(f, i) = (k < 2) ? o + 0.5 * kv[f] : (k == 2) ? o + kv[f] : o + (1.0 / 6.0) * a;
-          }
-        }
-        // ghost cells and passive ions return to Orig (their K is zero)
-        for (int w = tid; w < nc * (NF * 4 + NPAS * NPC); w += NT) {
+        // ghost cells and passive ions of the next buffer return to Orig
+        // (their K is zero)
+        {
           const int per = NF * 4 + NPAS * NPC;
-          const int cl = w / per, r = w - cl * per;
-          double* col = sm + size_t(L.stride) * cl;
-          if (r < NF * 4) {
-            const int f = r >> 2, u = r & 3;
-            const int g = (u < 2) ? u : nA + u;  // cells -1,0,nA+1,nA+2
-            col[L.X + f * G + g] = col[L.O + f * G + g];
-          } else {
-            col[L.XP + r - NF * 4] = col[L.OP + r - NF * 4];
+          const int nxpo = cur ? L.XP0 : L.XP1;
+          for (int w = tid; w < nc * per; w += NT) {
+            const int cl = w / per, r = w - cl * per;
+            double* col = sm + size_t(L.stride) * cl;
+            if (r < NF * 4) {
+              const int f = r >> 2, u = r & 3;
+              const int g = (u < 2) ? u : nA + u;  // cells -1,0,nA+1,nA+2
+              col[nxo + f * G + g] = col[L.O + f * G + g];
+            } else {
+              col[nxpo + r - NF * 4] = col[L.OP + r - NF * 4];
+            }
           }
         }
-        __syncthreads();  // @phase 4
-        if (k < 3) {
-          boundaries();
-          __syncthreads();  // @phase 1
-        }
+        cur ^= 1;
+        __syncthreads();  // @phase 3
+        // set_vertical_bcs on the updated state (:166,236,306,368)
+        boundaries();
+        __syncthreads();  // @phase 1
       }
-      // final set_vertical_bcs (:368-369)
-      boundaries();
-      __syncthreads();  // @phase 1
 
       // ---------------------------------------------------- store / reload
       const bool last = (step == kp.n_steps - 1);
@@ -880,10 +882,11 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         const int g = w / nc, cl = w - g * nc, i = g - 1;
         ColCtx c = ctx(cl);
         const bool store = last && sfrozen[cl] == 0u;
+        const bool pc = in_pcells(i, nA);
         if (IO == 1) {
           if (!store) continue;
           const GitmModVerticalBatch& b = M.mv;
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) {
             b.log_ns[gidx(s, g, cl)] = c.x(F_LNS + s, i);
             b.vert_vel[gidx(s, g, cl)] = c.x(F_W + s, i);
@@ -893,8 +896,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           b.vel_gd[gidx(1, g, cl)] = c.x(F_VN, i);
           b.vel_gd[gidx(2, g, cl)] = c.x(F_VU, i);
           b.log_rho[gidx(0, g, cl)] = c.x(F_LRHO, i);
-          const bool pc = in_pcells(i, nA);
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NI; ++s)
             if (s < NADV || pc) b.log_ins[gidx(s, g, cl)] = c.ion(s, i);
           continue;
@@ -905,14 +907,13 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         const double temperature = c.x(F_T, i) / c.tu(i);
         double nd[NS], N = 0.0;
         bool finite = isfinite(rho) && isfinite(temperature);
-        #pragma unroll
+#pragma unroll
         for (int s = 0; s < NS; ++s) {
           nd[s] = exp(c.x(F_LNS + s, i));
           N = N + nd[s];
           finite = finite && isfinite(nd[s]) && isfinite(c.x(F_W + s, i));
         }
         const bool improved = prm.use_improved_ion_advection != 0;
-        const bool pc = in_pcells(i, nA);
         const bool interior = (i >= 1 && i <= nA);
         if (store) {
           b.rho[gidx(0, g, cl)] = rho;
@@ -920,7 +921,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           b.velocity[gidx(1, g, cl)] = c.x(F_VN, i);
           b.velocity[gidx(2, g, cl)] = c.x(F_VU, i);
           b.temperature[gidx(0, g, cl)] = temperature;
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) {
             if (b.log_ns) b.log_ns[gidx(s, g, cl)] = c.x(F_LNS + s, i);
             b.vert_vel[gidx(s, g, cl)] = c.x(F_W + s, i);
@@ -929,7 +930,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           if (b.ndensity) b.ndensity[gidx(0, g, cl)] = N;
           if (prm.use_ion_advection) {
             double e = 0.0;
-            #pragma unroll
+#pragma unroll
             for (int s = 0; s < NI; ++s) {
               double v;
               if (s < NADV || pc) {
@@ -951,17 +952,17 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           // the next step's gather from the values just formed
           double gamma = c.gm(i), mmm = 0.0, tu = c.tu(i), cmx = c.cm(i);
           bool bad = false;
-          #pragma unroll
+#pragma unroll
           for (int s = 0; s < NS; ++s) bad = bad || !(nd[s] > 0.0);
           if (bad) atomicOr(&sst[cl], GITM_ST_NEG_DENSITY);
           if (prm.compute_coefficients) {
             double gg = 0.0;
-            #pragma unroll
+#pragma unroll
             for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
             gamma = gg * 2.0 / N + 1;
             double m = 0.0;
             const double rn = 1.0 / (N + 1.0);
-            #pragma unroll
+#pragma unroll
             for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
             if (m == 0) m = c_k.mass[0];
             mmm = m;
@@ -969,7 +970,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             cmx = 0.0;
             if (g >= 1 && g <= nA + 2) {
               double mx = fabs(c.x(F_W, i));
-              #pragma unroll
+#pragma unroll
               for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(c.x(F_W + s, i)));
               cmx = mx + sqrt(gamma * temperature);
             }
@@ -985,12 +986,12 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             if (i == -1) c.sc(SC_MMM_M1) = mmm;
             if (i == 0) c.sc(SC_MMM_0) = mmm;
           }
-                    // LogNS = log(NDensityS) and LogRho = log(Rho) of the next gather
+          // LogNS = log(NDensityS) and LogRho = log(Rho) of the next gather
           // (advance_vertical.f90:105,114) give back the values in X up to a
           // rounding of exp/log, so X keeps them
           c.x(F_T, i) = temperature * tu;
           if (prm.use_ion_advection) {
-            #pragma unroll
+#pragma unroll
             for (int s = 0; s < NI; ++s) {
               if (!(s < NADV || pc)) continue;
               double v = c.ion(s, i);
