@@ -815,6 +815,18 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     }
     dm[j] = d;
   }
+  // per-column grids must be on the device before the plan reads them
+  for (size_t j = 0; j < chunks.size(); ++j) {
+    const GitmColumnBatch& b = members[chunks[j].m];
+    if (!b.grid_per_column) continue;
+    const int G = b.n_alts + 4;
+    const size_t hp = size_t(b.n_cols) * sizeof(double), w = size_t(chunks[j].n) * sizeof(double);
+    const double* src[4] = {b.altitude, b.gravity, b.dalt_c, b.inv_r};
+    const double* dst[4] = {dm[j].altitude, dm[j].gravity, dm[j].dalt_c, dm[j].inv_r};
+    for (int q = 0; q < 4; ++q)
+      CUDA_TRY(ctx, cudaMemcpy2D(const_cast<double*>(dst[q]), w, src[q] + chunks[j].c0, hp, w, G,
+                                 cudaMemcpyHostToDevice));
+  }
   GitmVertPlan* P = nullptr;
   // plan_create checks that state arrays are device pointers: they are
   rc = gitm_vert_plan_create(ctx, dm.data(), int(dm.size()), &P);
@@ -845,6 +857,9 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     for (const ConstSpec& a : kInputs) {
       if (rc || !(d.*(a.field)) || !(b.*(a.field))) continue;
       if (d.*(a.field) == b.*(a.field)) continue;  // shared grid: read from the host at plan creation
+      const bool grid = (a.field == &GitmColumnBatch::altitude || a.field == &GitmColumnBatch::gravity ||
+                         a.field == &GitmColumnBatch::dalt_c || a.field == &GitmColumnBatch::inv_r);
+      if (grid) continue;  // per-column grid: copied before the plan was built
       if ((rc = h2d(const_cast<double*>(d.*(a.field)), b.*(a.field), rows_of(a.rows_per_cell, G)))) break;
     }
     if (rc) break;

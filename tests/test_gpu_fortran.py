@@ -108,6 +108,11 @@ def test_fortran_layout_matches_native(on_device):
         pytest.skip("no CUDA device")
     p = abi.default_params(compute_coefficients=0)
     m = synthetic.make_member(NLON * NLAT * NBLK, NALT, seed=41)
+    # CosLatitude(iLat, iBlock) is one value per latitude row
+    for b in range(NBLK):
+        for j in range(NLAT):
+            row = slice(b * 81 + j * 9, b * 81 + j * 9 + 9)
+            m.cos_lat[row] = m.cos_lat[b * 81 + j * 9]
     f = fortran_arrays(m)
     ns_in = f["ndensity_s"].copy()
     # native reference on the same columns
