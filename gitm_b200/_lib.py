@@ -36,6 +36,8 @@ SIGNATURES = {
                                            C.c_int]),
     "gitm_vert_advance_native_host": (C.c_int, [_P, C.POINTER(abi.GitmColumnBatch), C.c_int,
                                                 C.c_double, C.c_int]),
+    "gitm_vert_advance_native_noalloc": (C.c_int, [_P, C.POINTER(abi.GitmColumnBatch), C.c_double,
+                                                   C.c_int, _P, _P]),
     "gitm_vert_advance_1d": (C.c_int, [_P, C.POINTER(abi.GitmModVerticalBatch), C.c_double, _P]),
     "gitm_vert_cfl_dt": (C.c_int, [_P, C.POINTER(abi.GitmColumnBatch), C.c_int, C.c_double,
                                    C.c_double, C.c_double, C.POINTER(C.c_double)]),

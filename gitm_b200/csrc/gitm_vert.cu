@@ -1205,3 +1205,165 @@ extern "C" int gitm_vert_advance_fortran(GitmVertCtx* ctx, const GitmFortranStat
   ctx->params = saved;
   return rc;
 }
+
+// ------------------------------------------------------------------ no-allocation entry point
+// gitm_vert_advance_native_noalloc: the step of one member without any device
+// allocation, for callers that cannot allocate device memory while they run:
+// a GITM host whose memory is held by its own pool (a caching allocator that
+// has reserved the GPU), code issued while a CUDA stream is being captured
+// (cudaMalloc cannot be captured), and per-step loops that must not pay the
+// device synchronisation an allocation implies.  Everything the step needs
+// beyond the caller's inputs and outputs -- the member descriptor, the tile
+// list, the grid coefficients and the RK accumulators of the persistent CTAs
+// -- lives in the file-scope array below, which every GPU that loads this
+// library holds until the process exits.
+namespace {
+
+constexpr int64_t kNoAllocMaxCols = 262144;        // columns per call
+constexpr int kNoAllocThreads = 128;               // launch shape (accumulators in scratch)
+constexpr int kNoAllocSlots = 448;                 // persistent CTAs (>= 3 per SM on 148 SMs)
+constexpr size_t kNoAllocDescDoubles = 64;         // one DevMember
+constexpr size_t kNoAllocGridDoubles = 2048;       // NGC * G + NBC for G <= GITM_MAX_NALTS + 4
+constexpr size_t kNoAllocTileDoubles = size_t(kNoAllocMaxCols) * 2;  // one Tile (16 B) per column at most
+constexpr size_t kNoAllocAccDoubles = size_t(kNoAllocSlots) * NF * kNoAllocThreads;
+constexpr size_t kNoAllocDoubles =
+    kNoAllocDescDoubles + kNoAllocGridDoubles + kNoAllocTileDoubles + kNoAllocAccDoubles;  // 12.3 MiB
+static_assert(sizeof(DevMember) <= kNoAllocDescDoubles * sizeof(double), "descriptor slot too small");
+static_assert(size_t(NGC) * (GITM_MAX_NALTS + 4) + NBC <= kNoAllocGridDoubles, "grid slot too small");
+static_assert(sizeof(Tile) == 2 * sizeof(double), "tile size");
+
+// The shared scratch.  Calls that overlap on the GPU (on different streams,
+// or from different host threads) race on it: issue them in order.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// Device address of g_noalloc_scratch, looked up once per device on the
+// first call made with that device current (a host-side name of a __device__
+// variable is not its device address).
+static double* g_noalloc_addr[64] = {};
+
+// Builds the member descriptor, the grid coefficients of the member's
+// shared altitude grid (the formulas of grid_coefs above) and the tile list
+// in the scratch.  One CTA.
+__global__ void noalloc_setup_kernel(GitmColumnBatch b, int nc, int n_tiles, double* base) {
+  DevMember* dmem = reinterpret_cast<DevMember*>(base);
+  double* gridc = base + kNoAllocDescDoubles;
+  Tile* tiles = reinterpret_cast<Tile*>(base + kNoAllocDescDoubles + kNoAllocGridDoubles);
+  const int nA = b.n_alts, G = nA + 4;
+  if (threadIdx.x == 0) {
+    DevMember d;
+    memset(&d, 0, sizeof d);
+    d.b = b;
+    d.gridc = gridc;
+    d.gcols = 1;
+    d.col_offset = 0;
+    *dmem = d;
+    double dAF[GITM_MAX_NALTS + 4];
+    auto A = [&](int i) { return b.altitude[i + 1]; };
+    for (int i = 0; i <= nA + 2; ++i) dAF[i + 1] = A(i) - A(i - 1);
+    dAF[0] = dAF[1];
+    auto F = [&](int i) { return dAF[i + 1]; };
+    for (int g = 0; g < NGC * G + NBC; ++g) gridc[g] = 0.0;
+    for (int g = 0; g < G; ++g) {
+      const double idf = 1.0 / dAF[g];
+      gridc[GC_DALTF * G + g] = dAF[g];
+      gridc[GC_H2 * G + g] = idf * 2.0;
+      gridc[GC_IDF * G + g] = idf;
+      gridc[GC_IDC * G + g] = 1.0 / b.dalt_c[g];
+      gridc[GC_GRAV * G + g] = b.gravity[g];
+      gridc[GC_INVR * G + g] = b.inv_r[g];
+      gridc[GC_R * G + g] = 1.0 / b.inv_r[g];
+      gridc[GC_ALT * G + g] = b.altitude[g];
+    }
+    for (int i = 1; i <= nA; ++i) {
+      const double h1 = F(i - 1), h2 = F(i), h3 = F(i + 1), h4 = F(i + 2);
+      const double H2 = h2 + h1, H3 = h3 + h2 + h1, H4 = h4 + h3 + h2 + h1;
+      gridc[(GC_M0 + 0) * G + i + 1] = (h2 * h3 * (h3 + h4)) / (h1 * H2 * H3 * H4);
+      gridc[(GC_M0 + 1) * G + i + 1] = -1.0 * (H2 * h3 * (h3 + h4)) / (h1 * h2 * (h2 + h3) * (h2 + h3 + h4));
+      gridc[(GC_M0 + 2) * G + i + 1] =
+          (h2 * h3 * (h3 + h4) + H2 * h3 * (h3 + h4) - H2 * h2 * (h3 + h4) - H2 * h2 * h3) /
+          (H2 * h2 * h3 * (h3 + h4));
+      gridc[(GC_M0 + 3) * G + i + 1] = H2 * h2 * (h4 + h3) / (H3 * (h2 + h3) * h3 * h4);
+      gridc[(GC_M0 + 4) * G + i + 1] = -1.0 * H2 * h2 * h3 / (H4 * (h2 + h3 + h4) * (h3 + h4) * h4);
+    }
+    double* bc = gridc + NGC * G;
+    for (int k = 0; k < 2; ++k) {
+      const int iAlt = -k;
+      const double h1 = F(iAlt + 2), h2 = F(iAlt + 3), h3 = F(iAlt + 4), h4 = F(iAlt + 5);
+      const double M1 = h1, M2 = h1 + h2, M3 = h1 + h2 + h3, M4 = h1 + h2 + h3 + h4;
+      bc[5 * k + 0] = -1.0 * (M2 * M3 * M4 + M1 * M3 * M4 + M1 * M2 * M4 + M1 * M2 * M3) / (M1 * M2 * M3 * M4);
+      bc[5 * k + 1] = 1.0 * (M2 * M3 * M4) / (h1 * h2 * (h2 + h3) * (h2 + h3 + h4));
+      bc[5 * k + 2] = -1.0 * (M1 * M3 * M4) / (M2 * h2 * h3 * (h3 + h4));
+      bc[5 * k + 3] = 1.0 * (M1 * M2 * M4) / (M3 * (h3 + h2) * h3 * h4);
+      bc[5 * k + 4] = -1.0 * (M1 * M2 * M3) / (M4 * (h2 + h3 + h4) * (h3 + h4) * h4);
+    }
+    for (int k = 0; k < 2; ++k) {
+      const int iAlt = nA + 1 + k;
+      const double h1 = F(iAlt - 1), h2 = F(iAlt - 2), h3 = F(iAlt - 3), h4 = F(iAlt - 4);
+      const double M1 = h1, M2 = h1 + h2, M3 = h1 + h2 + h3, M4 = h1 + h2 + h3 + h4;
+      bc[10 + 5 * k + 0] = 1.0 * (M2 * M3 * M4 + M1 * M3 * M4 + M1 * M2 * M4 + M1 * M2 * M3) / (M1 * M2 * M3 * M4);
+      bc[10 + 5 * k + 1] = -1.0 * (M2 * M3 * M4) / (h1 * h2 * (h2 + h3) * (h2 + h3 + h4));
+      bc[10 + 5 * k + 2] = 1.0 * (M1 * M3 * M4) / (M2 * h2 * h3 * (h3 + h4));
+      bc[10 + 5 * k + 3] = -1.0 * (M1 * M2 * M4) / (M3 * (h3 + h2) * h3 * h4);
+      bc[10 + 5 * k + 4] = 1.0 * (M1 * M2 * M3) / (M4 * (h2 + h3 + h4) * (h3 + h4) * h4);
+    }
+  }
+  for (int t = threadIdx.x; t < n_tiles; t += blockDim.x) {
+    Tile tl;
+    tl.member = 0;
+    tl.c0 = int64_t(t) * nc;
+    tl.nc = int(min(int64_t(nc), b.n_cols - tl.c0));
+    tiles[t] = tl;
+  }
+}
+
+}  // namespace
+
+extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColumnBatch* member,
+                                                double dt, int n_steps, uint32_t* status_words,
+                                                void* stream) {
+  if (!ctx || !member || !status_words) return set_err(ctx, GITM_ERR_ARG, "ctx, member and status_words are required");
+  const GitmColumnBatch& b = *member;
+  int rc = check_member(ctx, b, ctx->params);
+  if (rc) return rc;
+  if (b.grid_per_column)
+    return set_err(ctx, GITM_ERR_ARG, "the no-allocation step takes one altitude grid per member (grid_per_column = 0)");
+  if (b.n_cols > kNoAllocMaxCols)
+    return set_err(ctx, GITM_ERR_ARG, "n_cols %lld exceeds the no-allocation limit of %lld columns per call",
+                   (long long)b.n_cols, (long long)kNoAllocMaxCols);
+  if (!(dt > 0.0)) return set_err(ctx, GITM_ERR_ARG, "dt must be > 0");
+  if (n_steps < 0) return set_err(ctx, GITM_ERR_ARG, "n_steps < 0");
+  if (b.n_cols == 0 || n_steps == 0) return GITM_OK;
+  if (ctx->device < 0 || ctx->device >= 64) return set_err(ctx, GITM_ERR_ARG, "device index out of range");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (!g_noalloc_addr[ctx->device]) {
+    void* p = nullptr;
+    CUDA_TRY(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[ctx->device] = static_cast<double*>(p);
+  }
+  double* base = g_noalloc_addr[ctx->device];
+  const int nA = b.n_alts;
+  int nc = std::min(kNoAllocThreads / nA, kNoAllocThreads / 32);
+  while (nc > 1 && smem_bytes(nA, nc) > ctx->max_smem) --nc;
+  nc = std::max(nc, 1);
+  const size_t smem = smem_bytes(nA, nc);
+  if (smem > ctx->max_smem) return set_err(ctx, GITM_ERR_ARG, "nAlts %d does not fit the no-allocation shape", nA);
+  const int n_tiles = int((b.n_cols + nc - 1) / nc);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(ctx, cudaMemsetAsync(status_words, 0, size_t(b.n_cols) * sizeof(uint32_t), st));
+  noalloc_setup_kernel<<<1, 128, 0, st>>>(b, nc, n_tiles, base);
+  CUDA_TRY(ctx, cudaGetLastError());
+  KParams kp;
+  kp.members = reinterpret_cast<const DevMember*>(base);
+  kp.tiles = reinterpret_cast<const Tile*>(base + kNoAllocDescDoubles + kNoAllocGridDoubles);
+  kp.n_tiles = n_tiles;
+  kp.n_steps = n_steps;
+  kp.dt = dt;
+  kp.status = status_words;
+  kp.scratch = base + kNoAllocDescDoubles + kNoAllocGridDoubles + kNoAllocTileDoubles;
+  kp.prm = ctx->params;
+  void* args[] = {&kp};
+  const int grid = std::min(n_tiles, kNoAllocSlots);
+  CUDA_TRY(ctx, cudaLaunchKernel((const void*)vert_step_kernel<0, kNoAllocThreads, 3, true>, dim3(grid),
+                                 dim3(kNoAllocThreads), args, smem, st));
+  return GITM_OK;
+}

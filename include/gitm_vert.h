@@ -244,6 +244,28 @@ int gitm_vert_advance_native(GitmVertCtx* ctx, const GitmColumnBatch* members,
 int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnBatch* members,
                                   int n_members, double dt, int n_steps);
 
+/* No counterpart in the reference.  n_steps RK4 steps of one member, like
+ * the plan API, but allocating no device memory: for callers that cannot
+ * allocate while they run -- a host whose GPU memory is held by its own pool,
+ * code issued during CUDA stream capture (cudaMalloc cannot be captured),
+ * and per-step loops that must not pay an allocation's device
+ * synchronisation.  Device pointers; asynchronous on `stream`.
+ *   - The member descriptor, tile list, grid coefficients and RK
+ *     accumulators live in one file-scope device array of 12.3 MiB that every
+ *     GPU loading the library holds until the process exits.
+ *   - Limits: n_cols <= 262144 and one altitude grid per member
+ *     (grid_per_column = 0); larger or per-column-grid members are rejected
+ *     with GITM_ERR_ARG.
+ *   - The first call on a device looks up the array's device address; make
+ *     that first call before any stream capture.
+ *   - Every call reuses the array, so calls that overlap on the GPU race:
+ *     issue them in order (one stream, or synchronise between streams).
+ *   - status_words (device, n_cols words) are zeroed and then receive each
+ *     column's GITM_ST_ bits; read them after the stream completes. */
+int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColumnBatch* member,
+                                     double dt, int n_steps, uint32_t* status_words,
+                                     void* stream);
+
 /* ---- ModVertical-form path --------------------------------------------- */
 
 /* One RK4 step of advance_vertical_1d_rusanov / _ausm (chosen by
