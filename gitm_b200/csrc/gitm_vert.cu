@@ -48,6 +48,7 @@ struct GitmVertPlan {
   int64_t n_cols_total = 0;
   int n_members = 0;
   int io = 0;  // 0 GITM arrays, 1 ModVertical arrays
+  int solver = GITM_SOLVER_RUSANOV;  // the context's solver when the plan was made
   GitmLaunchConfig cfg{256, 0, 1, 0};
   // tiles for the current cfg
   std::vector<Tile> tiles;
@@ -97,6 +98,7 @@ static void fill_consts(Consts& k) {
   for (int s = 0; s < NS; ++s) {
     k.mass[s] = mass[s];
     k.log_mass[s] = std::log(mass[s]);
+    k.log_kb = std::log(KB);
     k.k_over_m[s] = KB / mass[s];
     k.inv_vib2[s] = 1.0 / (vib[s] - 2);
     k.one_minus_e[s] = 1.0 - distinct[s];
@@ -116,8 +118,10 @@ static void fill_consts(Consts& k) {
 // dAlt_F / InvDAlt_F (advance_vertical.f90:149-151), the 5-point GradLogConS
 // mesh (vertical_solver_rusanov.f90:515-533) and the one-sided boundary
 // meshes (set_vertical_bcs.Earth.f90:279-297, 505-525).
+static size_t grid_rows(int G) { return size_t(NGC) * G + NBC + size_t(NGA) * G; }
+
 static void grid_coefs(int nA, const double* alt, const double* grav, const double* dalt_c,
-                       const double* inv_r, double* out /* [NGC*G + NBC] */) {
+                       const double* inv_r, double* out /* [grid_rows(G)] */) {
   const int G = nA + 4;
   std::vector<double> dAF(G), IDF(G);
   auto A = [&](int i) { return alt[i + 1]; };
@@ -125,7 +129,7 @@ static void grid_coefs(int nA, const double* alt, const double* grav, const doub
   dAF[0] = dAF[1];
   for (int g = 0; g < G; ++g) IDF[g] = 1.0 / dAF[g];
   auto F = [&](int i) { return dAF[i + 1]; };
-  std::fill(out, out + NGC * G + NBC, 0.0);
+  std::fill(out, out + grid_rows(G), 0.0);
   for (int g = 0; g < G; ++g) {
     out[GC_DALTF * G + g] = dAF[g];
     out[GC_H2 * G + g] = IDF[g] * 2.0;
@@ -169,6 +173,26 @@ static void grid_coefs(int nA, const double* alt, const double* grav, const doub
     bc[10 + 5 * k + 3] = -1.0 * (M1 * M2 * M4) / (M3 * (h3 + h2) * h3 * h4);
     bc[10 + 5 * k + 4] = 1.0 * (M1 * M2 * M3) / (M4 * (h2 + h3 + h4) * (h3 + h4) * h4);
   }
+  // AUSM cell constants: the Kp / Ku altitude profiles
+  // (vertical_solver_ausm.f90:1314-1352), the spherical face areas and cell
+  // volume (:2029-2039) and the wind-diffusion factor (:944-946)
+  double* ga = out + NGC * G + NBC;
+  const double LogMaxKu = std::log(0.50), LogMinKu = std::log(0.25);
+  const double LogMaxKp = std::log(1.0e-09), LogMinKp = std::log(1.0e-19);
+  const double KpWidth = 15.0e+03, KpAltMidPoint = 160.0e+03;
+  auto R = [&](int i) { return 1.0 / inv_r[i + 1]; };
+  for (int g = 0; g < G; ++g) ga[GA_DALTC * G + g] = dalt_c[g];
+  for (int i = 1; i <= nA; ++i) {
+    const double LeftRadius = 0.5 * (R(i) + R(i - 1));
+    const double RightRadius = 0.5 * (R(i) + R(i + 1));
+    ga[GA_AP * G + i + 1] = RightRadius * RightRadius;
+    ga[GA_AM * G + i + 1] = LeftRadius * LeftRadius;
+    ga[GA_VOL * G + i + 1] = (1.0 / 3.0) * (std::pow(RightRadius, 3.0) - std::pow(LeftRadius, 3.0));
+    const double th = std::tanh((A(i) - KpAltMidPoint) / KpWidth);
+    ga[GA_KP * G + i + 1] = std::exp(LogMinKp + 0.5 * (LogMaxKp - LogMinKp) * (1.0 + th));
+    ga[GA_KU * G + i + 1] = std::exp(LogMinKu + 0.5 * (LogMaxKu - LogMinKu) * (1.0 + th));
+    ga[GA_DAMP * G + i + 1] = 0.35 * std::exp(-1.0 * (A(i) - A(0)) / (45.0e+03));
+  }
 }
 
 // ------------------------------------------------------------------ kernels
@@ -187,17 +211,34 @@ static bool acc_global(int threads) {
   return false;
 }
 
-template <int IO>
-static const void* kernel_for(int threads) {
-  switch (threads) {
-    case 128: return (const void*)vert_step_kernel<IO, 128, 3, true>;
-    case 160: return (const void*)vert_step_kernel<IO, 160, 2, true>;
-    case 192: return (const void*)vert_step_kernel<IO, 192, 2, true>;
-    case 256: return (const void*)vert_step_kernel<IO, 256, 1, false>;
-    case 320: return (const void*)vert_step_kernel<IO, 320, 1, false>;
-    case 384: return (const void*)vert_step_kernel<IO, 384, 1, false>;
-    default: return nullptr;
+template <int IO, int SOLVER>
+static const void* kernel_for_t(int threads) {
+  if constexpr (SOLVER == GITM_SOLVER_AUSM) {
+    // the AUSM stage holds more state per cell: two shapes
+    switch (threads) {
+      case 128: return (const void*)vert_step_kernel<IO, 128, 2, true, SOLVER>;
+      case 256: return (const void*)vert_step_kernel<IO, 256, 1, false, SOLVER>;
+      default: return nullptr;
+    }
+  } else {
+    switch (threads) {
+      case 128: return (const void*)vert_step_kernel<IO, 128, 3, true, SOLVER>;
+      case 160: return (const void*)vert_step_kernel<IO, 160, 2, true, SOLVER>;
+      case 192: return (const void*)vert_step_kernel<IO, 192, 2, true, SOLVER>;
+      case 256: return (const void*)vert_step_kernel<IO, 256, 1, false, SOLVER>;
+      case 320: return (const void*)vert_step_kernel<IO, 320, 1, false, SOLVER>;
+      case 384: return (const void*)vert_step_kernel<IO, 384, 1, false, SOLVER>;
+      default: return nullptr;
+    }
   }
+}
+
+// The step kernel for an array form (0 GITM arrays, 1 ModVertical), solver
+// and CTA size, or nullptr when that shape is not built.
+static const void* kernel_for(int io, int solver, int threads) {
+  if (solver == GITM_SOLVER_AUSM)
+    return io ? kernel_for_t<1, GITM_SOLVER_AUSM>(threads) : kernel_for_t<0, GITM_SOLVER_AUSM>(threads);
+  return io ? kernel_for_t<1, GITM_SOLVER_RUSANOV>(threads) : kernel_for_t<0, GITM_SOLVER_RUSANOV>(threads);
 }
 
 // ------------------------------------------------------------------ API
@@ -227,8 +268,8 @@ void gitm_vert_default_params(GitmVertParams* p) {
 
 static int check_params(GitmVertCtx* ctx, const GitmVertParams* p) {
   if (!p) return set_err(ctx, GITM_ERR_ARG, "params is NULL");
-  if (p->solver != GITM_SOLVER_RUSANOV)
-    return set_err(ctx, GITM_ERR_UNSUPPORTED, "solver %d is not available in this build", p->solver);
+  if (p->solver != GITM_SOLVER_RUSANOV && p->solver != GITM_SOLVER_AUSM)
+    return set_err(ctx, GITM_ERR_ARG, "unknown solver %d", p->solver);
   if (!(p->beta_limiter >= 1.0 && p->beta_limiter <= 2.0))
     return set_err(ctx, GITM_ERR_ARG, "beta_limiter %g outside [1, 2]", p->beta_limiter);
   return GITM_OK;
@@ -260,10 +301,11 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
   Consts k;
   fill_consts(k);
   if (cudaMemcpyToSymbol(c_k, &k, sizeof k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
-  for (int t : kThreadChoices) {
-    cudaFuncSetAttribute(kernel_for<0>(t), cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem));
-    cudaFuncSetAttribute(kernel_for<1>(t), cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem));
-  }
+  for (int t : kThreadChoices)
+    for (int io = 0; io < 2; ++io)
+      for (int solver : {GITM_SOLVER_RUSANOV, GITM_SOLVER_AUSM})
+        if (const void* fn = kernel_for(io, solver, t))
+          cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem));
   *out = ctx;
   return GITM_OK;
 }
@@ -292,27 +334,27 @@ int gitm_vert_set_params(GitmVertCtx* ctx, const GitmVertParams* params) {
 }  // extern "C"
 
 // Columns per CTA for a member of nAlts under cfg.
-static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int nA) {
+static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int nA, int solver) {
   int nc = cfg.cols_per_cta > 0 ? cfg.cols_per_cta : cfg.threads / nA;
   nc = std::min(nc, cfg.threads / 32);  // one BC warp per column
   nc = std::min(nc, cfg.threads / nA);  // every interior cell has a thread
-  while (nc > 1 && smem_bytes(nA, nc) > ctx->max_smem) --nc;
+  while (nc > 1 && smem_bytes(nA, nc, solver) > ctx->max_smem) --nc;
   return std::max(nc, 1);
 }
 
 static int build_tiles(GitmVertPlan* P) {
   GitmVertCtx* ctx = P->ctx;
-  if (!kernel_for<0>(P->cfg.threads))
-    return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built (128..384)", P->cfg.threads);
+  if (!kernel_for(P->io, P->solver, P->cfg.threads))
+    return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built for solver %d", P->cfg.threads, P->solver);
   P->tiles.clear();
   P->smem = 0;
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnBatch& b = P->host_members[m];
-    const int nc = cols_per_cta(ctx, P->cfg, b.n_alts);
-    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc) > ctx->max_smem)
+    const int nc = cols_per_cta(ctx, P->cfg, b.n_alts, P->solver);
+    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc, P->solver) > ctx->max_smem)
       return set_err(ctx, GITM_ERR_ARG, "nAlts %d does not fit a CTA of %d threads", b.n_alts,
                      P->cfg.threads);
-    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc));
+    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc, P->solver));
     for (int64_t c0 = 0; c0 < b.n_cols; c0 += nc) {
       Tile t;
       t.member = m;
@@ -334,7 +376,7 @@ static int build_tiles(GitmVertPlan* P) {
   int grid = int(P->tiles.size());
   int per_sm = P->cfg.ctas_per_sm;
   if (acc_global(T) && per_sm <= 0) {
-    const void* fn = (P->io == 0) ? kernel_for<0>(T) : kernel_for<1>(T);
+    const void* fn = kernel_for(P->io, P->solver, T);
     CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->smem));
     per_sm = std::max(per_sm, 1);
   }
@@ -379,7 +421,7 @@ static int plan_common(GitmVertPlan* P, const double* const* alt, const double* 
     const int G = b.n_alts + 4;
     const int64_t gcols = gpc[m] ? b.n_cols : 1;
     goff[m] = gtotal;
-    gtotal += size_t(NGC * G + NBC) * gcols;
+    gtotal += grid_rows(G) * gcols;
   }
   CUDA_TRY(ctx, cudaMalloc(&P->d_grid, gtotal * sizeof(double)));
   for (int m = 0; m < P->n_members; ++m) {
@@ -392,7 +434,7 @@ static int plan_common(GitmVertPlan* P, const double* const* alt, const double* 
     CUDA_TRY(ctx, cudaMemcpy(hg.data(), grav[m], per * sizeof(double), cudaMemcpyDefault));
     CUDA_TRY(ctx, cudaMemcpy(hd.data(), dalt[m], per * sizeof(double), cudaMemcpyDefault));
     CUDA_TRY(ctx, cudaMemcpy(hi.data(), invr[m], per * sizeof(double), cudaMemcpyDefault));
-    std::vector<double> colv(NGC * G + NBC), out(size_t(NGC * G + NBC) * gcols);
+    std::vector<double> colv(grid_rows(G)), out(grid_rows(G) * gcols);
     std::vector<double> a1(G), g1(G), d1(G), i1(G);
     for (int64_t gc = 0; gc < gcols; ++gc) {
       for (int g = 0; g < G; ++g) {
@@ -402,7 +444,7 @@ static int plan_common(GitmVertPlan* P, const double* const* alt, const double* 
         i1[g] = hi[g * gcols + gc];
       }
       grid_coefs(nA, a1.data(), g1.data(), d1.data(), i1.data(), colv.data());
-      for (int r = 0; r < NGC * G + NBC; ++r) out[size_t(r) * gcols + gc] = colv[r];
+      for (size_t r = 0; r < grid_rows(G); ++r) out[r * gcols + gc] = colv[r];
     }
     CUDA_TRY(ctx, cudaMemcpy(P->d_grid + goff[m], out.data(), out.size() * sizeof(double),
                              cudaMemcpyHostToDevice));
@@ -460,6 +502,7 @@ int gitm_vert_plan_create(GitmVertCtx* ctx, const GitmColumnBatch* members, int 
   GitmVertPlan* P = new GitmVertPlan();
   P->ctx = ctx;
   P->io = 0;
+  P->solver = ctx->params.solver;
   P->n_members = n_members;
   P->host_members.assign(members, members + n_members);
   P->dev_members_host.resize(n_members);
@@ -527,7 +570,10 @@ static int launch_steps(GitmVertPlan* P, double dt, int n_steps, cudaStream_t st
   GitmVertCtx* ctx = P->ctx;
   if (P->tiles.empty() || n_steps <= 0) return GITM_OK;
   const int spl = std::max(1, P->cfg.steps_per_launch);
-  const void* fn = (P->io == 0) ? kernel_for<0>(P->cfg.threads) : kernel_for<1>(P->cfg.threads);
+  if (ctx->params.solver != P->solver)
+    return set_err(ctx, GITM_ERR_ARG, "plan was built for solver %d, context now selects %d", P->solver,
+                   ctx->params.solver);
+  const void* fn = kernel_for(P->io, P->solver, P->cfg.threads);
   if (!fn) return set_err(ctx, GITM_ERR_ARG, "no kernel for %d threads", P->cfg.threads);
   const int grid = P->grid;
   KParams kp;
@@ -836,7 +882,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
   for (int t = int(P->tiles.size()) - 1; t >= 0; --t) t0[P->tiles[t].member] = t;
   for (int j = int(chunks.size()) - 1; j >= 0; --j)
     if (t0[j] > t0[j + 1]) t0[j] = t0[j + 1];
-  const void* fn = kernel_for<0>(P->cfg.threads);
+  const void* fn = kernel_for(0, P->solver, P->cfg.threads);
   for (size_t j = 0; j < chunks.size() && !rc; ++j) {
     const Chunk& ch = chunks[j];
     const GitmColumnBatch& b = members[ch.m];
@@ -920,6 +966,7 @@ extern "C" int gitm_vert_advance_1d(GitmVertCtx* ctx, const GitmModVerticalBatch
   GitmVertPlan* P = new GitmVertPlan();
   P->ctx = ctx;
   P->io = 1;
+  P->solver = ctx->params.solver;
   P->n_members = 1;
   GitmColumnBatch shape;
   std::memset(&shape, 0, sizeof shape);
@@ -1327,6 +1374,8 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   if (rc) return rc;
   if (b.grid_per_column)
     return set_err(ctx, GITM_ERR_ARG, "the no-allocation step takes one altitude grid per member (grid_per_column = 0)");
+  if (ctx->params.solver != GITM_SOLVER_RUSANOV)
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "the no-allocation step runs the Rusanov solver only");
   if (b.n_cols > kNoAllocMaxCols)
     return set_err(ctx, GITM_ERR_ARG, "n_cols %lld exceeds the no-allocation limit of %lld columns per call",
                    (long long)b.n_cols, (long long)kNoAllocMaxCols);
@@ -1363,7 +1412,7 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   kp.prm = ctx->params;
   void* args[] = {&kp};
   const int grid = std::min(n_tiles, kNoAllocSlots);
-  CUDA_TRY(ctx, cudaLaunchKernel((const void*)vert_step_kernel<0, kNoAllocThreads, 3, true>, dim3(grid),
+  CUDA_TRY(ctx, cudaLaunchKernel((const void*)vert_step_kernel<0, kNoAllocThreads, 3, true, GITM_SOLVER_RUSANOV>, dim3(grid),
                                  dim3(kNoAllocThreads), args, smem, st));
   return GITM_OK;
 }

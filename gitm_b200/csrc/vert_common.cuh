@@ -44,6 +44,19 @@ enum GridCoef : int {
 };
 constexpr int NBC = 20;  // lower mesh coefs (cells 0,-1) x5, upper (nAlts+1,+2) x5
 
+// AUSM cell constants, [NGA][G][gcols] after the boundary block: they depend
+// on the grid only (vertical_solver_ausm.f90:944-946, 1314-1352, 2029-2039).
+enum AusmGridCoef : int {
+  GA_DALTC = 0,  // dAlt_C
+  GA_AP = 1,     // AreaFunction_P12 = RightRadius**2
+  GA_AM = 2,     // AreaFunction_M12 = LeftRadius**2
+  GA_VOL = 3,    // LocalCellVolume = (RightRadius**3 - LeftRadius**3) / 3
+  GA_KP = 4,     // LiouKpS
+  GA_KU = 5,     // Ku
+  GA_DAMP = 6,   // 0.35 exp(-(Altitude - Altitude(0)) / 45 km)
+  NGA = 7
+};
+
 // Earth constants (ModConstants.f90:11,15; ModEarth.f90:237-281,307-312).
 struct Consts {
   double mass[NS];
@@ -52,6 +65,7 @@ struct Consts {
   double inv_vib2[NS];           // 1 / (Vibration - 2)
   double kc[NS][NS];             // 1e-2 k / (Mass_i Diff0_ij): friction coefficient
   double one_minus_e[NS];        // the six distinct 1 - DiffExp values
+  double log_kb;                 // log(Boltzmanns_Constant)
 };
 
 struct DevMember {

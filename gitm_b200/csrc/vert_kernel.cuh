@@ -37,8 +37,11 @@ __device__ __forceinline__ int exp_index(int r, int q) {
 // ------------------------------------------------------------ smem layout
 struct Layout {
   int nAlts, G;
-  int X0, XP0, X1, XP1, O, OP, DL, TU, CM, GM, SC, stride;
+  int nsl;  // slope fields in DL: 18 (Rusanov) or 32 (AUSM)
+  int X0, XP0, X1, XP1, O, OP, DL, TU, CM, GM, SC, LT, QS, stride;
 };
+
+constexpr int NSLOPE_AUSM = 32;
 
 constexpr int NSC = 64;  // per-column scalars
 enum Scalar : int {
@@ -53,10 +56,11 @@ enum Scalar : int {
 // Per-column shared-memory slot (doubles): the stage state twice (a stage
 // reads one buffer and writes the next), Orig, the limited slopes, the
 // per-cell coefficients and the column scalars.
-__host__ __device__ inline Layout make_layout(int nAlts) {
+__host__ __device__ inline Layout make_layout(int nAlts, int solver = GITM_SOLVER_RUSANOV) {
   Layout L;
   L.nAlts = nAlts;
   L.G = nAlts + 4;
+  L.nsl = (solver == GITM_SOLVER_AUSM) ? NSLOPE_AUSM : NSTENCIL;
   const int G = L.G;
   int o = 0;
   L.X0 = o;  o += NF * G;
@@ -65,18 +69,21 @@ __host__ __device__ inline Layout make_layout(int nAlts) {
   L.XP1 = o; o += NPAS * NPC;
   L.O = o;   o += NF * G;
   L.OP = o;  o += NPAS * NPC;
-  L.DL = o;  o += NSTENCIL * (nAlts + 2);
+  L.DL = o;  o += L.nsl * (nAlts + 2);
   L.TU = o;  o += G;
   L.CM = o;  o += G;
   L.GM = o;  o += G;
   L.SC = o;  o += NSC;
+  // AUSM only: log T and the hydrostatic prefix sum of every cell
+  L.LT = o;  o += (solver == GITM_SOLVER_AUSM) ? G : 0;
+  L.QS = o;  o += (solver == GITM_SOLVER_AUSM) ? G : 0;
   L.stride = o;
   return L;
 }
 
 // Bytes of dynamic shared memory a tile of nc columns needs.
-__host__ __device__ inline size_t smem_bytes(int nAlts, int nc) {
-  Layout L = make_layout(nAlts);
+__host__ __device__ inline size_t smem_bytes(int nAlts, int nc, int solver = GITM_SOLVER_RUSANOV) {
+  Layout L = make_layout(nAlts, solver);
   return size_t(L.stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
 }
 
@@ -128,6 +135,10 @@ struct ColCtx {
     return __ldg(gridc + (size_t(NGC) * L.G + j) * gcols + gc);
   }
   __device__ __forceinline__ double dAF(int i) const { return g(GC_DALTF, i); }
+  // AUSM cell constant k at Fortran cell i
+  __device__ __forceinline__ double ga(int k, int i) const {
+    return __ldg(gridc + (size_t(NGC) * L.G + NBC + size_t(k) * L.G + (i + 1)) * gcols + gc);
+  }
 };
 
 // Sequential sum over lanes 0..n-1 of v (same order as a Fortran DO loop
@@ -412,6 +423,78 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
   __syncwarp();
 }
 
+// calc_neutral_friction (calc_neutral_friction.f90:47-106) for one cell:
+// solves (I + dt C) v = w in place and adds the eddy term -Eddy GradLogConS.
+// C_ij = 1e-2 k / (M_i D0_ij) n_j T^(1 - DiffExp_ij) (the NDensity factors of
+// the reference cancel); LU without pivoting, the matrix being strictly
+// diagonally dominant by rows.
+__device__ __forceinline__ void friction_solve(double dt, const double (&ns)[NS], double T, double eddy,
+                                               const double (&glc)[NS], double (&wv)[NS]) {
+  const double lt = log(T);
+  double pw[NS];
+#pragma unroll
+  for (int e = 0; e < NS; ++e) pw[e] = exp(c_k.one_minus_e[e] * lt);
+  double a[NS][NS];
+#pragma unroll
+  for (int r = 0; r < NS; ++r) {
+    double rs = 0.0;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      if (q == r) continue;
+      const double cij = c_k.kc[r][q] * ns[q] * pw[exp_index(r, q)];
+      a[r][q] = -dt * cij;
+      rs = rs + cij;
+    }
+    a[r][r] = 1.0 + dt * rs;
+  }
+#pragma unroll
+  for (int p = 0; p < NS; ++p) {
+    const double ip = 1.0 / a[p][p];
+    a[p][p] = ip;
+#pragma unroll
+    for (int r = p + 1; r < NS; ++r) {
+      const double l = a[r][p] * ip;
+#pragma unroll
+      for (int q = p + 1; q < NS; ++q) a[r][q] -= l * a[p][q];
+      wv[r] -= l * wv[p];
+    }
+  }
+#pragma unroll
+  for (int r = NS - 1; r >= 0; --r) {
+    double sum = wv[r];
+#pragma unroll
+    for (int q = r + 1; q < NS; ++q) sum -= a[r][q] * wv[q];
+    wv[r] = sum * a[r][r];
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) wv[s] = wv[s] + (-eddy * glc[s]);
+}
+
+// GradLogConS at cell i (vertical_solver_rusanov.f90:506-543,
+// vertical_solver_ausm.f90:644-686): the 5-point mesh on
+// LogConS = log(m_s) + LogNS - LogRho of the stage state.
+__device__ __forceinline__ void grad_log_cons(const ColCtx& c, int i, double (&glc)[NS]) {
+  double mc[5], lr5[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    mc[q] = c.g(GC_M0 + q, i);
+    lr5[q] = c.x(F_LRHO, i - 2 + q);
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) acc += mc[q] * (c_k.log_mass[s] + c.x(F_LNS + s, i - 2 + q) - lr5[q]);
+    glc[s] = acc;
+  }
+}
+
+}  // namespace gv
+
+#include "vert_ausm.cuh"
+
+namespace gv {
+
 // ------------------------------------------------------------ the kernel
 struct KParams {
   const DevMember* members;
@@ -432,7 +515,7 @@ constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
 // ACC_GLOBAL: the RK accumulator of each item lives in a per-CTA slot of
 // kp.scratch (coalesced, L2-resident under a persistent grid) instead of
 // registers, which lets small CTAs share an SM.
-template <int IO, int NT, int MINB, bool ACC_GLOBAL>
+template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER>
 __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
@@ -447,7 +530,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
     const DevMember& M = kp.members[tile.member];
     const int nA = M.b.n_alts;
     const int nc = tile.nc;
-    const Layout L = make_layout(nA);
+    const Layout L = make_layout(nA, SOLVER);
     const int G = L.G;
     const int64_t ncols = M.b.n_cols;
     uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(L.stride) * nc);  // [nc] status
@@ -661,30 +744,54 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
 
       for (int k = 0; k < 4; ++k) {
         // -------------------------------------------------- phase A
-        // limited slopes of the 18 swept fields on cells 0..nAlts+1
-        // (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772)
-        if (item) {
-          ColCtx c = ctx(my_cl);
-          const int i = my_i;
-          const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
-#pragma unroll 3
-          for (int f = 0; f < NSTENCIL; ++f) {
-            const double* v = &c.col[c.xo + f * G + 1];
-            const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-            const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-            c.dl(f, i) = limiter_mc(up, dn, prm.beta_limiter);
+        if constexpr (SOLVER == GITM_SOLVER_AUSM) {
+          // log T and the hydrostatic prefix sum of each column, then the 32
+          // limited slopes of the AUSM stage on cells 0..nAlts+1
+          constexpr int nw = NT / 32;
+          for (int cl = wid; cl < nc; cl += nw) {
+            ColCtx c = ctx(cl);
+            for (int i = lane - 1; i <= nA + 2; i += 32) c.col[L.LT + i + 1] = log(c.x(F_T, i));
+            __syncwarp();
+            ausm_prefix(c, lane);
           }
-        }
-        // the two end slopes of each column (:764-772)
-        for (int q = tid - nitems; q < nc * 2; q += NT) {
-          if (q < 0) continue;
-          const int cl = q >> 1;
-          ColCtx c = ctx(cl);
-          const int i = (q & 1) ? nA + 1 : 0;
-          const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
-          for (int f = 0; f < NSTENCIL; ++f) {
-            const double* v = &c.col[c.xo + f * G + 1];
-            c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, prm.beta_limiter);
+          __syncthreads();  // @phase 6
+          if (item) {
+            ColCtx c = ctx(my_cl);
+#pragma unroll 4
+            for (int f = 0; f < NSLOPE_AUSM; ++f) c.dl(f, my_i) = ausm_slope(c, f, my_i, prm.beta_limiter);
+          }
+          for (int q = tid - nitems; q < nc * 2; q += NT) {
+            if (q < 0) continue;
+            ColCtx c = ctx(q >> 1);
+            const int i = (q & 1) ? nA + 1 : 0;
+            for (int f = 0; f < NSLOPE_AUSM; ++f) c.dl(f, i) = ausm_slope(c, f, i, prm.beta_limiter);
+          }
+        } else {
+          // limited slopes of the 18 swept fields on cells 0..nAlts+1
+          // (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772)
+          if (item) {
+            ColCtx c = ctx(my_cl);
+            const int i = my_i;
+            const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+#pragma unroll 3
+            for (int f = 0; f < NSTENCIL; ++f) {
+              const double* v = &c.col[c.xo + f * G + 1];
+              const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+              const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
+              c.dl(f, i) = limiter_mc(up, dn, prm.beta_limiter);
+            }
+          }
+          // the two end slopes of each column (:764-772)
+          for (int q = tid - nitems; q < nc * 2; q += NT) {
+            if (q < 0) continue;
+            const int cl = q >> 1;
+            ColCtx c = ctx(cl);
+            const int i = (q & 1) ? nA + 1 : 0;
+            const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+            for (int f = 0; f < NSTENCIL; ++f) {
+              const double* v = &c.col[c.xo + f * G + 1];
+              c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, prm.beta_limiter);
+            }
           }
         }
         __syncthreads();  // @phase 2
@@ -699,158 +806,123 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           const int i = my_i;
           double* xn = c.col + nxo + 1;  // next buffer, xn[f*G + i]
           auto emit = [&](int f, double kval) {
-            double a;
-            if constexpr (ACC_GLOBAL) {
-              double& ag = accg[size_t(f) * NT];
-              a = (k == 0) ? kval : (k < 3) ? ag + 2.0 * kval : ag + kval;
-              ag = a;
+            const int fa = ACC_GLOBAL ? 0 : f;
+            const double prev = ACC_GLOBAL ? accg[size_t(f) * NT] : accr[fa];
+            const double o = c.o(f, i);
+            double a, x1;
+            if constexpr (SOLVER == GITM_SOLVER_AUSM) {
+              // Stage(k+2) = Stage1 + (New - state), and the final combination
+              // (1/3)(-Stage1 + Stage2 + 2 Stage3 + Stage4 + (New - state))
+              // accumulated in the reference's order (vertical_solver_ausm.f90:167-189,381-420)
+              if (k < 3) {
+                x1 = o + kval;
+                a = (k == 0) ? -1.0 * o + x1 : (k == 1) ? prev + 2.0 * x1 : prev + x1;
+              } else {
+                a = prev;
+                x1 = (1.0 / 3.0) * (prev + kval);
+              }
             } else {
-              const int fa = ACC_GLOBAL ? 0 : f;
-              a = (k == 0) ? kval : (k < 3) ? accr[fa] + 2.0 * kval : accr[fa] + kval;
+              a = (k == 0) ? kval : (k < 3) ? prev + 2.0 * kval : prev + kval;
+              x1 = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
+            }
+            if constexpr (ACC_GLOBAL) {
+              accg[size_t(f) * NT] = a;
+            } else {
               accr[fa] = a;
             }
-            const double o = c.o(f, i);
-            xn[f * G + i] = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
+            xn[f * G + i] = x1;
           };
-          const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
-          const double idc = c.g(GC_IDC, i);
-          const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
-          const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
-          // calc_rusanov_alts_rusanov (:694-718) at cell i
-          auto sweep = [&](int f, double& grad, double& diff) {
-            const double* v = &c.col[c.xo + f * G + 1];
-            const double* d = &c.col[L.DL + f * (nA + 2)];
-            const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
-            const double R0 = v[i] - 0.5 * d[i] * dF0;
-            const double L1 = v[i] + 0.5 * d[i] * dF1;
-            const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
-            grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
-            diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
-          };
-          const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
-          const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
-          double gT, dT;
-          sweep(F_T, gT, dT);
-          {
-            double gE, dE, gN, dN, gU, dU;
-            sweep(F_VE, gE, dE);
-            sweep(F_VN, gN, dN);
-            sweep(F_VU, gU, dU);
-            // :660-680
-            emit(F_VE, (VE - dt * VU * gE + dt * dE) - VE);
-            emit(F_VN, (VN - dt * VU * gN + dt * dN) - VN);
-            const double divv = gU + 2 * VU * invr;
-            emit(F_T, (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T);
-          }
-          // ions 1..nIonsAdvect (:557-568)
-#pragma unroll
-          for (int s = 0; s < NADV; ++s) {
-            double gI, dI;
-            sweep(F_I + s, gI, dI);
-            const double I = c.x(F_I + s, i);
-            emit(F_I + s, (I - dt * (ivup * gI) + dt * dI) - I);
-          }
-          // species continuity and momentum (:548-617)
-          const double itau = 1.0 / (prm.use_damping
-                                         ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
-                                         : prm.vert_tau);
-          const double hz = (VN * VN + VE * VE) * invr;
-          const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
-          double wv[NS];
-          double sumrho = 0.0;
-#pragma unroll
-          for (int s = 0; s < NS; ++s) {
-            double gL, dL, gW, dW;
-            sweep(F_LNS + s, gL, dL);
-            sweep(F_W + s, gW, dW);
-            const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
-            const double divw = gW + 2 * Ws * invr;
-            const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
-            emit(F_LNS + s, nl - Ls);
-            sumrho = sumrho + c_k.mass[s] * exp(nl);
-            const double km = c_k.k_over_m[s];
-            double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
-            w = w + cor;
-            w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
-            wv[s] = w;
-          }
-          const double LR = c.x(F_LRHO, i);
-          emit(F_LRHO, log(sumrho) - LR);
-          // NS = exp(LogNS), 1 / Rho (:466-467)
-          double ns[NS];
-#pragma unroll
-          for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
-          const double ir = exp(-LR);
-          // calc_neutral_friction (calc_neutral_friction.f90:47-106)
-          if (prm.use_neutral_friction) {
-            // GradLogConS (:506-543), LogConS = log(m_s) + LogNS - LogRho
-            double glc[NS];
+          if constexpr (SOLVER == GITM_SOLVER_AUSM) {
+            // advance_vertical_1stage_ausm with DtIn = Dt/2, Dt/2, Dt, Dt/2
+            ausm_cell(c, i, prm, (k == 2) ? dt : 0.5 * dt, eddy, ivup, emit);
+          } else {
+            const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
+            const double idc = c.g(GC_IDC, i);
+            const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
+            const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
+            // calc_rusanov_alts_rusanov (:694-718) at cell i
+            auto sweep = [&](int f, double& grad, double& diff) {
+              const double* v = &c.col[c.xo + f * G + 1];
+              const double* d = &c.col[L.DL + f * (nA + 2)];
+              const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
+              const double R0 = v[i] - 0.5 * d[i] * dF0;
+              const double L1 = v[i] + 0.5 * d[i] * dF1;
+              const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
+              grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+              diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
+            };
+            const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
+            const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
+            double gT, dT;
+            sweep(F_T, gT, dT);
             {
-              double mc[5], lr5[5];
-#pragma unroll
-              for (int q = 0; q < 5; ++q) {
-                mc[q] = c.g(GC_M0 + q, i);
-                lr5[q] = c.x(F_LRHO, i - 2 + q);
-              }
-#pragma unroll
-              for (int s = 0; s < NS; ++s) {
-                double acc = 0.0;
-#pragma unroll
-                for (int q = 0; q < 5; ++q)
-                  acc += mc[q] * (c_k.log_mass[s] + c.x(F_LNS + s, i - 2 + q) - lr5[q]);
-                glc[s] = acc;
-              }
+              double gE, dE, gN, dN, gU, dU;
+              sweep(F_VE, gE, dE);
+              sweep(F_VN, gN, dN);
+              sweep(F_VU, gU, dU);
+              // :660-680
+              emit(F_VE, (VE - dt * VU * gE + dt * dE) - VE);
+              emit(F_VN, (VN - dt * VU * gN + dt * dN) - VN);
+              const double divv = gU + 2 * VU * invr;
+              emit(F_T, (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T);
             }
-            const double lt = log(T);
-            double pw[NS];
+            // ions 1..nIonsAdvect (:557-568)
 #pragma unroll
-            for (int e = 0; e < NS; ++e) pw[e] = exp(c_k.one_minus_e[e] * lt);
-            double a[NS][NS];
-#pragma unroll
-            for (int r = 0; r < NS; ++r) {
-              double rs = 0.0;
-#pragma unroll
-              for (int q = 0; q < NS; ++q) {
-                if (q == r) continue;
-                const double cij = c_k.kc[r][q] * ns[q] * pw[exp_index(r, q)];
-                a[r][q] = -dt * cij;
-                rs = rs + cij;
-              }
-              a[r][r] = 1.0 + dt * rs;
+            for (int s = 0; s < NADV; ++s) {
+              double gI, dI;
+              sweep(F_I + s, gI, dI);
+              const double I = c.x(F_I + s, i);
+              emit(F_I + s, (I - dt * (ivup * gI) + dt * dI) - I);
             }
-            // LU without pivoting (the matrix is strictly row diagonally dominant)
+            // species continuity and momentum (:548-617)
+            const double itau = 1.0 / (prm.use_damping
+                                           ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
+                                           : prm.vert_tau);
+            const double hz = (VN * VN + VE * VE) * invr;
+            const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
+            double wv[NS];
+            double sumrho = 0.0;
 #pragma unroll
-            for (int p = 0; p < NS; ++p) {
-              const double ip = 1.0 / a[p][p];
-              a[p][p] = ip;
-#pragma unroll
-              for (int r = p + 1; r < NS; ++r) {
-                const double l = a[r][p] * ip;
-#pragma unroll
-                for (int q = p + 1; q < NS; ++q) a[r][q] -= l * a[p][q];
-                wv[r] -= l * wv[p];
-              }
+            for (int s = 0; s < NS; ++s) {
+              double gL, dL, gW, dW;
+              sweep(F_LNS + s, gL, dL);
+              sweep(F_W + s, gW, dW);
+              const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
+              const double divw = gW + 2 * Ws * invr;
+              const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
+              emit(F_LNS + s, nl - Ls);
+              sumrho = sumrho + c_k.mass[s] * exp(nl);
+              const double km = c_k.k_over_m[s];
+              double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
+              w = w + cor;
+              w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
+              wv[s] = w;
             }
+            const double LR = c.x(F_LRHO, i);
+            emit(F_LRHO, log(sumrho) - LR);
+            // NS = exp(LogNS), 1 / Rho (:466-467)
+            double ns[NS];
 #pragma unroll
-            for (int r = NS - 1; r >= 0; --r) {
-              double sum = wv[r];
-#pragma unroll
-              for (int q = r + 1; q < NS; ++q) sum -= a[r][q] * wv[q];
-              wv[r] = sum * a[r][r];
+            for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
+            const double ir = exp(-LR);
+            // calc_neutral_friction (calc_neutral_friction.f90:47-106)
+            if (prm.use_neutral_friction) {
+              // GradLogConS (:506-543), LogConS = log(m_s) + LogNS - LogRho
+              double glc[NS];
+              grad_log_cons(c, i, glc);
+              friction_solve(dt, ns, T, eddy, glc, wv);
             }
+            // clamp and bulk vertical wind (:643-658)
+            double vu = 0.0;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) wv[s] = wv[s] + (-eddy * glc[s]);
+            for (int s = 0; s < NS; ++s) {
+              double w = fmax(-prm.max_vertical_velocity, wv[s]);
+              w = fmin(prm.max_vertical_velocity, w);
+              emit(F_W + s, w - c.x(F_W + s, i));
+              vu = vu + w * (c_k.mass[s] * ns[s] * ir);
+            }
+            emit(F_VU, vu - VU);
           }
-          // clamp and bulk vertical wind (:643-658)
-          double vu = 0.0;
-#pragma unroll
-          for (int s = 0; s < NS; ++s) {
-            double w = fmax(-prm.max_vertical_velocity, wv[s]);
-            w = fmin(prm.max_vertical_velocity, w);
-            emit(F_W + s, w - c.x(F_W + s, i));
-            vu = vu + w * (c_k.mass[s] * ns[s] * ir);
-          }
-          emit(F_VU, vu - VU);
         }
         // ghost cells and passive ions of the next buffer return to Orig
         // (their K is zero)

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "gitm_vert_oracle.hpp"
+#include "oracle_ausm.hpp"
 #include "flop_counter.hpp"
 
 using namespace gvo;
@@ -28,7 +29,10 @@ inline double grid_at(const double* p, int g, int64_t c, const GitmColumnBatch& 
 
 template <class R>
 void run_solver(Column<R>& col, const GitmVertParams& prm, double dt) {
-  advance_vertical_1d_rusanov(col, prm, dt);
+  if (prm.solver == GITM_SOLVER_AUSM)
+    advance_vertical_1d_ausm(col, prm, dt);
+  else
+    advance_vertical_1d_rusanov(col, prm, dt);
 }
 
 // One column of one member through n_steps steps (producers, gather, RK4,

@@ -30,6 +30,12 @@ CASES = {
                                     dict(use_improved_ion_advection=0, use_neutral_friction=0,
                                          use_nighttime_ion_bcs=0), {}),
     "rusanov_given_coefficients": (6, 50, 15, 1, 2.0, dict(compute_coefficients=0), {}),
+    "ausm_default": (8, 50, 16, 1, 2.0, dict(solver=abi.SOLVER_AUSM), {}),
+    "ausm_2steps_log_ions_nofriction": (6, 30, 17, 2, 2.0,
+                                        dict(solver=abi.SOLVER_AUSM, use_neutral_friction=0,
+                                             use_improved_ion_advection=0), {}),
+    "ausm_msis_nocoriolis": (6, 40, 18, 1, 2.0, dict(solver=abi.SOLVER_AUSM, use_msis_bcs=1, use_coriolis=0),
+                             dict(with_lbc=True)),
 }
 
 
@@ -56,6 +62,7 @@ def save(name):
 
 if __name__ == "__main__":
     oracle.build()
-    for name in CASES:
+    names = sys.argv[1:] or list(CASES)
+    for name in names:
         save(name)
         print("wrote", name)

@@ -56,3 +56,18 @@ def test_noalloc_rejects_oversized_member():
                                                       C.c_void_p(status.data_ptr()), None)
     assert rc == abi.ERR_ARG
     assert "262144" in ctx.last_error()
+
+
+def test_noalloc_rejects_ausm():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gitm_b200 import _lib
+    from gitm_b200 import vertical as V
+    ctx = V.VerticalContext(abi.default_params(solver=abi.SOLVER_AUSM))
+    m = V.device_member(synthetic.make_member(4, 50, seed=63))
+    b = m.batch()
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    rc = _lib.lib().gitm_vert_advance_native_noalloc(ctx.handle, C.byref(b), 2.0, 1,
+                                                      C.c_void_p(status.data_ptr()), None)
+    assert rc == abi.ERR_UNSUPPORTED
