@@ -8,6 +8,10 @@ Inputs are seeded synthetic columns (gitm_b200/synthetic.py); the state
 (about 0.9 GB) is larger than L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--solver rusanov|ausm]
+
+The default solver is Rusanov (GITM's default, UseAUSMSolver = F); `--solver
+ausm` measures the AUSM solver on the same workload.
 
 Under torchrun (N > 1) every rank advances its own globe (an ensemble member
 seeded by rank): weak scaling, no data exchange in the timed loop.
@@ -50,7 +54,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--plain-steps", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--solver", default="rusanov", choices=["rusanov", "ausm"])
     return ap.parse_args()
+
+
+SOLVER_NAMES = {"rusanov": "Rusanov RK4", "ausm": "AUSM RK4"}
+
+
+def solver_params(name: str, **over):
+    from gitm_b200 import abi
+    return abi.default_params(solver=abi.SOLVER_AUSM if name == "ausm" else abi.SOLVER_RUSANOV, **over)
 
 
 def dist_env():
@@ -112,10 +125,10 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- helpers
-def opcount(n_alts: int) -> float:
+def opcount(n_alts: int, solver: str = "rusanov") -> float:
     with open(os.path.join(ROOT, "tests", "golden", "opcount.json")) as f:
         d = json.load(f)
-    return float(d["rusanov"][str(n_alts)]["flop_eq_per_column_step"])
+    return float(d[solver][str(n_alts)]["flop_eq_per_column_step"])
 
 
 def profile_traffic():
@@ -161,15 +174,14 @@ def measure_fp64_peak(torch, device) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_baseline(m, seconds: float, threads: int | None = None) -> dict:
+def cpu_baseline(m, seconds: float, threads: int | None = None, solver: str = "rusanov") -> dict:
     """The oracle (CPU restatement of the reference) on the host cores on a
     bounded sample: the first S columns of the globe, one step each call."""
-    from gitm_b200 import abi
     from gitm_b200.parallel import shard_member
     from oracle import oracle
 
     threads = threads or os.cpu_count() or 1
-    p = abi.default_params()
+    p = solver_params(solver)
     probe = shard_member(m, 0, max(1, m.n_cols // (64 * threads)))
     t0 = time.perf_counter()
     oracle.advance(probe.copy(), p, DT, 1, nthreads=threads)
@@ -197,7 +209,7 @@ def run_reference(args):
     per_step = max(per_step, 1.0)
     cb = None
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(m, min(per_step, 10.0))
+        cb = cpu_baseline(m, min(per_step, 10.0), solver=args.solver)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = statistics.median(vals) if vals else cb["value"]
@@ -207,7 +219,7 @@ def run_reference(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded)",
            "config": {"workload": f"globe {args.deg} deg, {m.n_cols} columns x {args.n_alts} alts, "
-                                  "Rusanov RK4, dt 2 s",
+                                  f"{SOLVER_NAMES[args.solver]}, dt 2 s",
                       "parallelism": "host threads"},
            "cpu_baseline": cb,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -231,7 +243,7 @@ def run_ours(args):
 
     m = synthetic.globe_member(args.deg, args.deg, n_alts=args.n_alts, seed=rank)
     n_cols = m.n_cols
-    p = abi.default_params()
+    p = solver_params(args.solver)
     ctx = V.VerticalContext(p, device=local)
     dm = V.device_member(m, device=dev)
     plan = V.Plan(ctx, [dm])
@@ -352,7 +364,7 @@ def run_ours(args):
                       "stepped, copied out (chunked, overlapped); wall clock"}
 
     if rank == 0:
-        flops_cs = opcount(args.n_alts)
+        flops_cs = opcount(args.n_alts, args.solver)
         n_launch = max(1, launches)
         t_launch = el / n_launch
         cs_launch = n_cols * steps_done / n_launch
@@ -364,7 +376,7 @@ def run_ours(args):
             pass
         bytes_cs = algorithmic_bytes_per_column_step(args.n_alts) / max(1, cfg.steps_per_launch)
         achieved = flops_cs * cs_launch / t_launch / 1e12
-        traffic = profile_traffic()
+        traffic = profile_traffic() if args.solver == "rusanov" else None
         roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak,
                 "traffic": None if traffic is None else traffic * cs_launch,
@@ -377,13 +389,13 @@ def run_ours(args):
             ach = bytes_cs * n_cols * steps_done / el / 1e9
             hbm = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                    "frac": ach / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
-        cb = cpu_baseline(m, args.cpu_seconds) if args.cpu_seconds > 0 else None
+        cb = cpu_baseline(m, args.cpu_seconds, solver=args.solver) if args.cpu_seconds > 0 else None
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                "steps": steps_done, "warmup": args.warmup,
                "ms_per_step": 1e3 * el / steps_done, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                "config": {"workload": f"globe {args.deg} deg, {n_cols} columns x {args.n_alts} alts "
-                                      "per GPU, Rusanov RK4, dt 2 s",
+                                      f"per GPU, {SOLVER_NAMES[args.solver]}, dt 2 s",
                           "columns_per_gpu": n_cols, "n_alts": args.n_alts,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                           "l2": "state larger than L2 (no flush needed)",

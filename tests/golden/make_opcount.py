@@ -33,10 +33,11 @@ def count(n_alts=50, seed=1, **over):
 
 def main():
     out = {"convention": "add/sub/mul/div/sqrt = 1, transcendental = %d" % TRANS_FLOPS,
-           "rusanov": {}}
-    for n_alts in (50, 75, 100):
-        ops, flops = count(n_alts)
-        out["rusanov"][str(n_alts)] = {"ops": ops, "flop_eq_per_column_step": flops}
+           "rusanov": {}, "ausm": {}}
+    for name, solver in (("rusanov", abi.SOLVER_RUSANOV), ("ausm", abi.SOLVER_AUSM)):
+        for n_alts in (50, 75, 100):
+            ops, flops = count(n_alts, solver=solver)
+            out[name][str(n_alts)] = {"ops": ops, "flop_eq_per_column_step": flops}
     with open(os.path.join(HERE, "opcount.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     print(json.dumps(out, indent=1))
