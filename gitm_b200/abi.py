@@ -112,6 +112,8 @@ class GitmColumnBatch(C.Structure):
         ("gravity", _dp),
         ("dalt_c", _dp),
         ("inv_r", _dp),
+        ("heating", _dp),
+        ("heating_scale", _dp),
     ]
 
 

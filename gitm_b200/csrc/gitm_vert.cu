@@ -790,6 +790,7 @@ const ConstSpec kInputs[] = {
     {&GitmColumnBatch::mlat, 0},      {&GitmColumnBatch::lbc, -1},
     {&GitmColumnBatch::altitude, 1},  {&GitmColumnBatch::gravity, 1},
     {&GitmColumnBatch::dalt_c, 1},    {&GitmColumnBatch::inv_r, 1},
+    {&GitmColumnBatch::heating, 1},   {&GitmColumnBatch::heating_scale, 0},
 };
 
 inline int64_t rows_of(int rpc, int G) { return rpc > 0 ? int64_t(rpc) * G : (rpc == 0 ? 1 : 2 * GITM_LBC_NVALUES); }

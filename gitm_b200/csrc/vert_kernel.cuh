@@ -976,7 +976,13 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         // scatter, advance_vertical.f90:163-217
         const GitmColumnBatch& b = M.b;
         const double rho = store ? exp(c.x(F_LRHO, i)) : 1.0;
-        const double temperature = c.x(F_T, i) / c.tu(i);
+        double temperature = c.x(F_T, i) / c.tu(i);
+        // add_sources' temperature line with EuvHeating its only term
+        // (add_sources.f90:53-66), applied after every step
+        if (IO == 0 && M.b.heating && i >= 1 && i <= nA) {
+          const double hs = M.b.heating_scale ? M.b.heating_scale[tile.c0 + cl] : 1.0;
+          temperature = temperature + dt * (hs * M.b.heating[gidx(0, g, cl)]);
+        }
         double nd[NS], N = 0.0;
         bool finite = isfinite(rho) && isfinite(temperature);
 #pragma unroll

@@ -197,6 +197,8 @@ class Member:
     lbc: np.ndarray | None = None
     log_ns: np.ndarray | None = None
     ndensity: np.ndarray | None = None
+    heating: np.ndarray | None = None
+    heating_scale: np.ndarray | None = None
 
     STATE = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel")
     COEFFS = ("gamma", "mean_major_mass", "temp_unit", "cmax")
@@ -239,7 +241,7 @@ def smooth_profiles(rng, alt: np.ndarray, n_cols: int, n_modes: int = 6,
 
 def make_member(n_cols: int, n_alts: int = 50, seed: int = 0, tinf_shift: float = 0.0,
                 lat_deg: np.ndarray | None = None, with_lbc: bool = False,
-                with_outputs: bool = True) -> Member:
+                with_outputs: bool = True, with_heating: bool = False) -> Member:
     rng = np.random.Generator(np.random.PCG64(seed))
     G = n_alts + 4
     alt = make_altitude_grid(n_alts)
@@ -317,6 +319,14 @@ def make_member(n_cols: int, n_alts: int = 50, seed: int = 0, tinf_shift: float 
     if with_outputs:
         m.log_ns = np.zeros((NSPECIES, G, n_cols))
         m.ndensity = np.zeros((1, G, n_cols))
+    if with_heating:
+        # EUV heating: 1e-8 K/s at 100 km scaled by rho(100 km) / rho(z), in
+        # the normalised units of Temperature (K/s / TempUnit), with a
+        # lognormal (sigma 0.3) factor per column; a separate random stream
+        # keeps the other fields identical with and without heating
+        hr = np.random.Generator(np.random.PCG64([seed, 1]))
+        m.heating = (1.0e-8 * rho[2][None, :] / rho / tu)[None].copy()
+        m.heating_scale = np.exp(hr.normal(0.0, 0.3, n_cols))
     return m
 
 

@@ -97,7 +97,8 @@ class VerticalContext:
 # ------------------------------------------------------------------ members
 FIELDS = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel", "log_ns",
           "ndensity", "gamma", "mean_major_mass", "temp_unit", "cmax", "ivel_up", "eddy",
-          "cos_lat", "sza", "mlat", "lbc", "altitude", "gravity", "dalt_c", "inv_r")
+          "cos_lat", "sza", "mlat", "lbc", "altitude", "gravity", "dalt_c", "inv_r", "heating",
+          "heating_scale")
 
 
 @dataclasses.dataclass
@@ -268,7 +269,7 @@ def advance_vertical_all_host(ctx: VerticalContext, members, dt: float, n_steps:
 
 MODVERT_FIELDS = ("log_rho", "temp", "vel_gd", "log_ns", "vert_vel", "log_ins", "ivel", "cmax",
                   "mean_major_mass", "gamma", "eddy", "centrifugal", "coriolis", "sza", "mlat",
-                  "lbc", "altitude", "gravity", "dalt_c", "inv_r")
+                  "lbc", "altitude", "gravity", "dalt_c", "inv_r", "heating", "heating_scale")
 
 
 def advance_vertical_1d(ctx: VerticalContext, cols: dict, dt: float):

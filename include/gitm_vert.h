@@ -118,6 +118,12 @@ typedef struct GitmVertParams {
  *   altitude, gravity, dalt_c, inv_r: Altitude_GB, Gravity_GB, dAlt_GB,
  *        InvRadialDistance_GB -- [G] when grid_per_column = 0, [G][n_cols]
  *        when grid_per_column = 1.
+ * Optional heating update after each step (may be NULL):
+ *   heating         EuvHeating (normalised K/s, cells 1..nAlts are used)
+ *   heating_scale   [n_cols] factor on heating per column (NULL = 1)
+ *   With heating set, every step ends with the temperature line of
+ *   add_sources (add_sources.f90:53-66) with EuvHeating as its only nonzero
+ *   term: Temperature(1:nAlts) += dt * heating_scale * heating.
  */
 typedef struct GitmColumnBatch {
   int32_t n_alts;
@@ -145,6 +151,8 @@ typedef struct GitmColumnBatch {
   const double* gravity;
   const double* dalt_c;
   const double* inv_r;
+  const double* heating;
+  const double* heating_scale;
 } GitmColumnBatch;
 
 /*

@@ -133,6 +133,9 @@ uint32_t step_gitm_column(const GitmVertParams& prm, const GitmColumnBatch& m, i
       m.rho[nat(0, g, c, G, n)] = rho;
       for (int d = 0; d < 3; ++d) m.velocity[nat(d, g, c, G, n)] = col.Vel_GD[d * G + g];
       double T = col.Temp[g] / tu[g];
+      // add_sources.f90:53-66 with EuvHeating its only nonzero term
+      if (m.heating && g - 1 >= 1 && g - 1 <= nAlts)
+        T = T + dt * ((m.heating_scale ? m.heating_scale[c] : 1.0) * m.heating[nat(0, g, c, G, n)]);
       m.temperature[nat(0, g, c, G, n)] = T;
       finite = finite && std::isfinite(rho) && std::isfinite(T);
       double N = 0.0;

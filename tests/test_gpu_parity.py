@@ -68,6 +68,16 @@ def test_step_matches_oracle(torch_cuda, oracle_lib, variant):
     np.testing.assert_array_equal(st, st_ref)
 
 
+@pytest.mark.parametrize("n_steps", [1, 4])
+def test_heating_update(torch_cuda, oracle_lib, n_steps):
+    """The add_sources temperature line after each step, resident steps included."""
+    p = abi.default_params()
+    m = synthetic.make_member(64, 50, seed=34, with_heating=True)
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0, n_steps=n_steps)
+    out, _ = gpu_advance(m, p, 2.0, n_steps=n_steps, config=dict(steps_per_launch=n_steps))
+    assert_state_close(out, ref, STATE, rtol=1e-10 if n_steps == 1 else 1e-9)
+
+
 def test_msis_lower_boundary(torch_cuda, oracle_lib):
     p = abi.default_params(use_msis_bcs=1)
     m = synthetic.make_member(64, 50, seed=22, with_lbc=True)

@@ -122,3 +122,20 @@ def test_operation_count(oracle_lib):
     flops = ops["add"] + ops["mul"] + ops["div"] + ops["sqrt"] + 20 * ops["trans"]
     # a few hundred thousand flop-equivalents per column-step
     assert 2e5 < flops < 2e6, ops
+
+
+def test_oracle_heating_update(oracle_lib):
+    """add_sources' temperature line: interior cells gain dt * scale * heating."""
+    from gitm_b200 import abi, synthetic
+    m = synthetic.make_member(8, 50, seed=3, with_heating=True)
+    m0 = synthetic.make_member(8, 50, seed=3)
+    p = abi.default_params()
+    a, b = m.copy(), m0.copy()
+    oracle_lib.advance(a, p, 2.0, 1)
+    oracle_lib.advance(b, p, 2.0, 1)
+    d = a.temperature - b.temperature
+    want = 2.0 * (m.heating_scale[None, None, :] * m.heating)
+    # the difference of two temperatures: exact to a few ulps of T
+    np.testing.assert_allclose(d[0, 2:-2], want[0, 2:-2], rtol=1e-9,
+                               atol=4e-16 * np.abs(b.temperature).max())
+    assert np.abs(d[0, [0, 1, -2, -1]]).max() == 0.0
