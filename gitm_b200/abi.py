@@ -26,6 +26,7 @@ ST_NEG_ION_TOP = 2
 ST_LU_SINGULAR = 4
 ST_NONFINITE = 8
 ST_BAD_NALTS = 16
+ST_ADJ_BRANCH = 32
 
 SOLVER_RUSANOV = 0
 SOLVER_AUSM = 1
@@ -113,6 +114,21 @@ class GitmColumnBatch(C.Structure):
         ("dalt_c", _dp),
         ("inv_r", _dp),
         ("heating", _dp),
+        ("heating_scale", _dp),
+    ]
+
+
+class GitmColumnAdjoint(C.Structure):
+    _fields_ = [
+        ("ndensity_s", _dp),
+        ("idensity_s", _dp),
+        ("rho", _dp),
+        ("temperature", _dp),
+        ("velocity", _dp),
+        ("vert_vel", _dp),
+        ("log_ns", _dp),
+        ("ndensity", _dp),
+        ("eddy", _dp),
         ("heating_scale", _dp),
     ]
 

@@ -1,0 +1,176 @@
+"""Gradients through the vertical step: the adjoint kernel
+(gitm_vert_plan_adjoint) behind torch.autograd.
+
+GITM has no adjoint; this module adds reverse-mode differentiation of the
+step of advance_vertical_all (Rusanov solver, GITM-array form) for
+sensitivity studies and data assimilation:
+
+* ``StepRunner`` holds one member's device arrays and a plan; ``step`` runs
+  one forward step, ``vjp`` one adjoint step.
+* ``vertical_step(runner, state, eddy, heating_scale)`` is one step as a
+  differentiable torch op (``torch.autograd.Function``).
+* ``rollout(runner, state, n_steps, every, eddy, heating_scale)`` is an
+  ``n_steps`` rollout that keeps only every ``every``-th state in memory and
+  recomputes the states of a segment when its adjoint runs (checkpointing),
+  each adjoint step re-running its own stages on the GPU.
+* ``o_n2_objective`` is the column-weighted log(n_O / n_N2) at one altitude
+  level.
+
+The state is the GITM arrays the step reads and writes: NDensityS,
+IDensityS, Rho, Temperature (normalised), Velocity, VerticalVelocity, as
+[field, cell, column] float64 CUDA tensors.  All compute goes through
+libgitmvert.so.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import synthetic
+from . import vertical as V
+
+STATE = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel")
+
+
+class StepRunner:
+    """One member's arrays and a plan over them; the state arrays are
+    overwritten by every call."""
+
+    def __init__(self, ctx: V.VerticalContext, member, dt: float):
+        self.ctx = ctx
+        self.dt = float(dt)
+        self.dm = V.device_member(member) if isinstance(member, synthetic.Member) else member
+        if self.dm.tensors.get("heating") is not None and self.dm.tensors.get("heating_scale") is None:
+            self.dm.tensors["heating_scale"] = torch.ones(self.dm.n_cols, dtype=torch.float64,
+                                                          device=self.dm.tensors["rho"].device)
+        self.plan = V.Plan(ctx, [self.dm])
+
+    @property
+    def tensors(self):
+        return self.dm.tensors
+
+    def _load(self, state, eddy=None, heating_scale=None):
+        for k in STATE:
+            self.dm.tensors[k].copy_(state[k])
+        if eddy is not None:
+            self.dm.tensors["eddy"].copy_(eddy)
+        if heating_scale is not None and self.dm.tensors.get("heating_scale") is not None:
+            self.dm.tensors["heating_scale"].copy_(heating_scale)
+
+    def state(self) -> dict:
+        return {k: self.dm.tensors[k].clone() for k in STATE}
+
+    def step(self, state, eddy=None, heating_scale=None) -> dict:
+        """One forward step from `state`; returns the new state (copies)."""
+        self._load(state, eddy, heating_scale)
+        self.plan.advance(self.dt, 1)
+        return self.state()
+
+    def vjp(self, state, ybar, eddy=None, heating_scale=None):
+        """Adjoint of one step taken from `state`: returns (xbar, eddy_bar,
+        heating_scale_bar).  ybar: dict of output adjoints (None = zero)."""
+        self._load(state, eddy, heating_scale)
+        bars = {}
+        for k in STATE:
+            y = ybar.get(k)
+            bars[k] = torch.zeros_like(self.dm.tensors[k]) if y is None else y.detach().clone().contiguous()
+        for k in ("log_ns", "ndensity"):
+            if ybar.get(k) is not None:
+                bars[k] = ybar[k].detach().contiguous()
+        bars["eddy"] = torch.zeros_like(self.dm.tensors["eddy"])
+        hs = self.dm.tensors.get("heating_scale")
+        bars["heating_scale"] = None if hs is None else torch.zeros_like(hs)
+        self.plan.adjoint([bars], self.dt)
+        return {k: bars[k] for k in STATE}, bars["eddy"], bars["heating_scale"]
+
+    def check(self):
+        self.plan.check()
+
+    def close(self):
+        self.plan.close()
+
+
+class _Step(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, runner, eddy, heating_scale, *state):
+        out = runner.step(dict(zip(STATE, state)), eddy, heating_scale)
+        ctx.runner = runner
+        ctx.save_for_backward(eddy, heating_scale, *state)
+        return tuple(out[k] for k in STATE)
+
+    @staticmethod
+    def backward(ctx, *ybar):
+        eddy, hs, *state = ctx.saved_tensors
+        xbar, eb, hb = ctx.runner.vjp(dict(zip(STATE, state)), dict(zip(STATE, ybar)), eddy, hs)
+        return (None, eb, hb, *[xbar[k] for k in STATE])
+
+
+def vertical_step(runner: StepRunner, state: dict, eddy=None, heating_scale=None) -> dict:
+    """One step as a differentiable op; eddy / heating_scale default to the
+    runner's arrays (then not differentiated)."""
+    if eddy is None:
+        eddy = runner.tensors["eddy"].clone()
+    if heating_scale is None:
+        hs = runner.tensors.get("heating_scale")
+        heating_scale = torch.ones(1, device=eddy.device, dtype=eddy.dtype) if hs is None else hs.clone()
+    out = _Step.apply(runner, eddy, heating_scale, *[state[k] for k in STATE])
+    return dict(zip(STATE, out))
+
+
+class _Rollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, runner, n_steps, every, eddy, heating_scale, *state):
+        s = dict(zip(STATE, (t.detach() for t in state)))
+        ckpts = []
+        for t in range(n_steps):
+            if t % every == 0:
+                ckpts.append({k: v.clone() for k, v in s.items()})
+            s = runner.step(s, eddy, heating_scale)
+        ctx.runner, ctx.n_steps, ctx.every, ctx.ckpts = runner, n_steps, every, ckpts
+        ctx.save_for_backward(eddy, heating_scale)
+        return tuple(s[k] for k in STATE)
+
+    @staticmethod
+    def backward(ctx, *ybar):
+        eddy, hs = ctx.saved_tensors
+        runner = ctx.runner
+        y = dict(zip(STATE, ybar))
+        eb = torch.zeros_like(eddy)
+        hb = torch.zeros_like(hs)
+        n, k = ctx.n_steps, ctx.every
+        for seg in reversed(range(len(ctx.ckpts))):
+            t0 = seg * k
+            t1 = min(t0 + k, n)
+            states = [ctx.ckpts[seg]]
+            for _ in range(t0, t1 - 1):
+                states.append(runner.step(states[-1], eddy, hs))
+            for st in reversed(states):
+                y, e, h = runner.vjp(st, y, eddy, hs)
+                eb += e
+                if h is not None and hb.shape == h.shape:
+                    hb += h
+            ctx.ckpts[seg] = None
+        return (None, None, None, eb, hb, *[y[k2] for k2 in STATE])
+
+
+def rollout(runner: StepRunner, state: dict, n_steps: int, every: int = 10, eddy=None,
+            heating_scale=None) -> dict:
+    """n_steps steps with checkpoints every `every` steps (see module doc)."""
+    if eddy is None:
+        eddy = runner.tensors["eddy"].clone()
+    if heating_scale is None:
+        hs = runner.tensors.get("heating_scale")
+        heating_scale = torch.ones(1, device=eddy.device, dtype=eddy.dtype) if hs is None else hs.clone()
+    out = _Rollout.apply(runner, int(n_steps), max(1, int(every)), eddy, heating_scale,
+                         *[state[k] for k in STATE])
+    return dict(zip(STATE, out))
+
+
+def o_n2_objective(ndensity_s, weights, level: int):
+    """sum_c w_c log(n_O / n_N2) at cell index `level` (0 = cell -1)."""
+    return (weights * (torch.log(ndensity_s[0, level]) - torch.log(ndensity_s[2, level]))).sum()
+
+
+def level_of(altitude, alt_m: float) -> int:
+    """Cell index (0 = cell -1) whose altitude is closest to alt_m."""
+    a = torch.as_tensor(altitude).reshape(-1)
+    return int(torch.argmin((a - alt_m).abs()))

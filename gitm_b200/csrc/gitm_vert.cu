@@ -18,6 +18,7 @@
 
 #include "vert_common.cuh"
 #include "vert_kernel.cuh"
+#include "vert_adjoint.cuh"
 
 using namespace gv;
 
@@ -58,6 +59,15 @@ struct GitmVertPlan {
   double* d_scratch = nullptr;  // RK accumulators of persistent CTAs
   size_t scratch_doubles = 0;
   int max_nalts = 0, min_nalts = 1 << 30;
+  // adjoint launch (built on the first gitm_vert_plan_adjoint)
+  bool adj_ready = false;
+  std::vector<Tile> adj_tiles;
+  Tile* d_adj_tiles = nullptr;
+  size_t adj_smem = 0;
+  int adj_grid = 0, adj_nc_max = 0, adj_per_max = 0;
+  size_t adj_scratch_per_cta = 0;
+  double* d_adj_scratch = nullptr;
+  GitmColumnAdjoint* d_bars = nullptr;
 };
 
 static int set_err(GitmVertCtx* ctx, int code, const char* fmt, ...) {
@@ -466,6 +476,9 @@ static int plan_common(GitmVertPlan* P, const double* const* alt, const double* 
 
 static void plan_free(GitmVertPlan* P) {
   if (!P) return;
+  cudaFree(P->d_adj_tiles);
+  cudaFree(P->d_adj_scratch);
+  cudaFree(P->d_bars);
   cudaFree(P->d_scratch);
   cudaFree(P->d_members);
   cudaFree(P->d_grid);
@@ -730,6 +743,97 @@ extern "C" int gitm_vert_advance_native(GitmVertCtx* ctx, const GitmColumnBatch*
   plan_free(P);
   if (!rc && st) rc = set_err(ctx, GITM_ERR_COLUMN, "%lld columns reported status 0x%x", (long long)nbad, st);
   return rc;
+}
+
+// ------------------------------------------------------------------ adjoint
+constexpr int kAdjThreads = 128;
+
+// Tiles, persistent grid and scratch of the adjoint kernel for the plan.
+static int adjoint_prepare(GitmVertPlan* P) {
+  GitmVertCtx* ctx = P->ctx;
+  if (P->adj_ready) return GITM_OK;
+  const int T = kAdjThreads;
+  P->adj_tiles.clear();
+  P->adj_smem = 0;
+  P->adj_nc_max = 1;
+  P->adj_per_max = 0;
+  for (int m = 0; m < P->n_members; ++m) {
+    const GitmColumnBatch& b = P->host_members[m];
+    const int nA = b.n_alts;
+    int nc = std::max(1, std::min(T / nA, T / 32));
+    while (nc > 1 && adj_smem_bytes(nA, nc) > ctx->max_smem) --nc;
+    if (nA > T || adj_smem_bytes(nA, nc) > ctx->max_smem)
+      return set_err(ctx, GITM_ERR_UNSUPPORTED, "adjoint: nAlts %d does not fit a CTA of %d threads", nA, T);
+    P->adj_smem = std::max(P->adj_smem, adj_smem_bytes(nA, nc));
+    P->adj_nc_max = std::max(P->adj_nc_max, nc);
+    P->adj_per_max = std::max(P->adj_per_max, adj_state_doubles(nA));
+    for (int64_t c0 = 0; c0 < b.n_cols; c0 += nc) {
+      Tile t;
+      t.member = m;
+      t.nc = int(std::min<int64_t>(nc, b.n_cols - c0));
+      t.c0 = c0;
+      P->adj_tiles.push_back(t);
+    }
+  }
+  if (P->adj_tiles.empty()) {
+    P->adj_ready = true;
+    return GITM_OK;
+  }
+  const void* fn = (const void*)vert_adjoint_kernel<kAdjThreads>;
+  CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem)));
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->adj_smem));
+  per_sm = std::max(per_sm, 1);
+  P->adj_grid = int(std::min<size_t>(P->adj_tiles.size(), size_t(per_sm) * ctx->num_sms));
+  P->adj_scratch_per_cta = size_t(ADJ_NSTATE) * P->adj_nc_max * P->adj_per_max + size_t(2) * NF * T;
+  CUDA_TRY(ctx, cudaMalloc(&P->d_adj_tiles, P->adj_tiles.size() * sizeof(Tile)));
+  CUDA_TRY(ctx, cudaMemcpy(P->d_adj_tiles, P->adj_tiles.data(), P->adj_tiles.size() * sizeof(Tile),
+                           cudaMemcpyHostToDevice));
+  if (cudaMalloc(&P->d_adj_scratch, size_t(P->adj_grid) * P->adj_scratch_per_cta * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, GITM_ERR_NOMEM, "adjoint: cannot allocate the stage-state scratch");
+  }
+  CUDA_TRY(ctx, cudaMalloc(&P->d_bars, std::max(1, P->n_members) * sizeof(GitmColumnAdjoint)));
+  P->adj_ready = true;
+  return GITM_OK;
+}
+
+extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* bars, double dt, void* stream) {
+  if (!P) return GITM_ERR_ARG;
+  GitmVertCtx* ctx = P->ctx;
+  if (!bars && P->n_members > 0) return set_err(ctx, GITM_ERR_ARG, "bars is NULL");
+  if (!(dt > 0.0)) return set_err(ctx, GITM_ERR_ARG, "dt must be > 0");
+  if (P->io != 0) return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint takes GITM-array plans");
+  if (P->solver != GITM_SOLVER_RUSANOV || ctx->params.solver != GITM_SOLVER_RUSANOV)
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint differentiates the Rusanov solver");
+  for (int m = 0; m < P->n_members; ++m) {
+    const GitmColumnAdjoint& a = bars[m];
+    if (!a.ndensity_s || !a.idensity_s || !a.rho || !a.temperature || !a.velocity || !a.vert_vel)
+      return set_err(ctx, GITM_ERR_ARG, "member %d: the state adjoint arrays are required", m);
+  }
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  int rc = adjoint_prepare(P);
+  if (rc) return rc;
+  if (P->adj_tiles.empty()) return GITM_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(ctx, cudaMemcpyAsync(P->d_bars, bars, P->n_members * sizeof(GitmColumnAdjoint),
+                                cudaMemcpyHostToDevice, st));
+  AParams kp;
+  kp.members = P->d_members;
+  kp.bars = P->d_bars;
+  kp.tiles = P->d_adj_tiles;
+  kp.n_tiles = int(P->adj_tiles.size());
+  kp.nc_max = P->adj_nc_max;
+  kp.per_max = P->adj_per_max;
+  kp.dt = dt;
+  kp.status = P->d_status;
+  kp.scratch = P->d_adj_scratch;
+  kp.scratch_per_cta = P->adj_scratch_per_cta;
+  kp.prm = ctx->params;
+  void* args[] = {&kp};
+  CUDA_TRY(ctx, cudaLaunchKernel((const void*)vert_adjoint_kernel<kAdjThreads>, dim3(P->adj_grid),
+                                 dim3(kAdjThreads), args, P->adj_smem, st));
+  return GITM_OK;
 }
 
 // ------------------------------------------------------------------ staging

@@ -1,0 +1,1246 @@
+// vert_adjoint.cuh -- reverse-mode derivative of one vertical step (Rusanov
+// solver, GITM-array form): gitm_vert_plan_adjoint.
+//
+// The reference has no adjoint; this is the hand-written reverse of the
+// forward kernel of vert_kernel.cuh, statement by statement, with every
+// branch (limiter case, clamp, boundary switch, max of |w|) differentiated on
+// the side the forward took.
+//
+// One CTA per tile of columns, persistent over tiles.  The CTA first re-runs
+// the step forward (gather, producers, boundaries, four stages) and saves
+// the six states it needs -- the gathered state, the post-boundary stage
+// inputs X0..X3 and the final X4 -- to a per-CTA slot of global scratch
+// (L2-resident under the persistent grid).  The reverse sweep then runs from
+// the scatter back to the gather:
+//   scatter^T -> bc^T(X4) -> RK combination^T -> for k = 3..0:
+//     load X_k, recompute its slopes, stage_k^T at every interior cell
+//     (neighbour contributions by shared-memory atomics), slopes^T,
+//     bc^T(X_k) and the combination^T of X_k
+//   -> bc^T(X0) -> gather^T and producers^T.
+// Shared memory per column: the state, its adjoint, the adjoint of Orig, the
+// slopes and their adjoints, the per-cell coefficients and their adjoints.
+#pragma once
+
+#include "vert_kernel.cuh"
+
+namespace gv {
+
+struct AdjLayout {
+  Layout L;  // X0: the state; X1: its adjoint; O: the adjoint of Orig
+  int DB, CMB, GMB, TUB, MMB, stride;
+};
+
+__host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
+  AdjLayout A;
+  A.L = make_layout(nAlts);
+  const int G = nAlts + 4;
+  int o = A.L.stride;
+  A.DB = o;  o += NSTENCIL * (nAlts + 2);
+  A.CMB = o; o += G;
+  A.GMB = o; o += G;
+  A.TUB = o; o += G;
+  A.MMB = o; o += 4;  // MeanMajorMass at cells -1, 0; the heating-factor sum
+  A.stride = o;
+  return A;
+}
+
+__host__ __device__ inline size_t adj_smem_bytes(int nAlts, int nc) {
+  return size_t(make_adj_layout(nAlts).stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
+}
+
+constexpr int ADJ_NSTATE = 6;  // gathered state, X0, X1, X2, X3, X4
+__host__ __device__ inline int adj_state_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
+
+struct AParams {
+  const DevMember* members;
+  const GitmColumnAdjoint* bars;
+  const Tile* tiles;
+  int n_tiles;
+  int nc_max;
+  int per_max;             // adj_state_doubles of the largest member
+  double dt;
+  uint32_t* status;
+  double* scratch;
+  size_t scratch_per_cta;  // doubles
+  GitmVertParams prm;
+};
+
+// ---------------------------------------------------------------- helpers
+// Adjoint of limiter_mc: (ub, db) from the output adjoint ob, on the branch
+// limiter_mc takes for (u, d).
+__device__ __forceinline__ void limiter_mc_adjoint(double u, double d, double beta, double ob, double& ub,
+                                                   double& db) {
+  ub = 0.0;
+  db = 0.0;
+  const double bu = beta * u, bd = beta * d, av = (u + d) * 0.5;
+  if (u > 0.0) {
+    if (d > 0.0) {
+      const double m = fmin(bu, bd);
+      if (m <= av) {
+        if (bu <= bd) ub = beta * ob; else db = beta * ob;
+      } else {
+        ub = 0.5 * ob;
+        db = 0.5 * ob;
+      }
+    }
+  } else if (d < 0.0) {
+    const double m = fmax(bu, bd);
+    if (m >= av) {
+      if (bu >= bd) ub = beta * ob; else db = beta * ob;
+    } else {
+      ub = 0.5 * ob;
+      db = 0.5 * ob;
+    }
+  }
+}
+
+// Per-column view of the adjoint arrays in shared memory.
+struct ColAdj {
+  double* xb;    // adjoint of the state, [f*G + cell+1]
+  double* xbp;   // its passive-ion cells
+  double* ob;    // adjoint of Orig
+  double* obp;
+  double* db;    // slope adjoints [f*(nAlts+2) + cell]
+  double* cmb;   // cMax adjoint [cell+1]
+  double* gmb;   // Gamma adjoint
+  double* tub;   // TempUnit adjoint
+  double* mmb;   // MeanMajorMass(-1), MeanMajorMass(0), heating-factor sum
+  int G, nA;
+
+  __device__ __forceinline__ double& x(int f, int i) const { return xb[f * G + i + 1]; }
+  __device__ __forceinline__ double& ion(int s, int i) const {
+    return (s < NADV) ? xb[(F_I + s) * G + i + 1] : xbp[(s - NADV) * NPC + pcell(i, nA)];
+  }
+  __device__ __forceinline__ void add(int f, int i, double v) const { atomicAdd(&xb[f * G + i + 1], v); }
+  __device__ __forceinline__ void dadd(int f, int c, double v) const { atomicAdd(&db[f * (nA + 2) + c], v); }
+};
+
+// ---------------------------------------------------------------- boundaries^T
+// Reverse of bc_column for one column, by one thread.  c: the post-boundary
+// state; a: its adjoint, replaced by the adjoint of the pre-boundary state
+// (ghost cells the boundary overwrites get 0, ghost cells it reads before
+// overwriting get their contribution); pre / prep: the pre-boundary state's
+// cells and passive-ion cells (the values of ion ghosts the top boundary
+// reads).  Follows set_vertical_bcs.Earth.f90:8-652 as bc_column does.
+__device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const double* pre,
+                                         const double* prep, const GitmVertParams& prm, uint32_t* st) {
+  const int nA = c.L.nAlts;
+  const int G = c.L.G;
+  const double* sc = c.col + c.L.SC;
+  auto X = [&](int f, int i) -> double { return c.x(f, i); };
+  auto XI = [&](int s, int i) -> double { return c.ion(s, i); };
+  auto PI = [&](int s, int i) -> double {
+    return (s < NADV) ? pre[(F_I + s) * G + i + 1] : prep[(s - NADV) * NPC + pcell(i, nA)];
+  };
+  const double* bl = sc + SC_BCC;       // lower mesh coefficients: cell 0 then -1
+  const double* bu = sc + SC_BCC + 10;  // upper: nA+1 then nA+2
+  auto dAF = [&](int i) { return c.dAF(i); };
+
+  // ================= upper boundary, reversed
+  // lines 598-604: LogRho of the two top ghosts
+  for (int cc = nA + 1; cc <= nA + 2; ++cc) {
+    double ms[NS], r = 0.0;
+    for (int s = 0; s < NS; ++s) {
+      ms[s] = c_k.mass[s] * exp(X(F_LNS + s, cc));
+      r = r + ms[s];
+    }
+    const double lb = a.x(F_LRHO, cc);
+    a.x(F_LRHO, cc) = 0.0;
+    for (int s = 0; s < NS; ++s) a.x(F_LNS + s, cc) += lb * ms[s] / r;
+  }
+  // lines 488-596: ions
+  {
+    const bool improved = prm.use_improved_ion_advection != 0;
+    double tp = 0.0;
+    for (int i = 1; i <= nA; ++i) tp += c.dAF(i) * (improved ? XI(0, i) : exp(XI(0, i)));
+    const bool hold = (tp / 1e16 < prm.min_tec) && (sc[SC_PLASMA] != 0.0);
+    bool neg = false;
+    if (improved)
+      for (int s = 0; s < NI; ++s)
+        for (int q = nA - 5; q <= nA + 2; ++q) {
+          const double v = (q >= nA + 1) ? PI(s, q) : XI(s, q);
+          neg = neg || (v < 0.0);
+        }
+    if (neg) {
+      atomicOr(st, GITM_ST_ADJ_BRANCH);
+    } else if (!hold) {
+      const double dT = dAF(nA);
+      for (int s = 0; s < NI; ++s) {
+        if (improved) {
+          double n[6];
+          n[0] = log(PI(s, nA + 1));
+          for (int j = 1; j < 6; ++j) n[j] = log(XI(s, nA + 1 - j));
+          const double* C = bu;
+          const double dnr = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
+          const double lim = -(0.001 * n[0] / dT);
+          const bool t1 = dnr > lim;
+          const double dn = t1 ? lim : dnr;
+          const double v1 = exp(n[1] + dn * dAF(nA + 1));
+          const double g0 = log(PI(s, nA + 2));
+          const double nn1 = log(v1);
+          const double* D = bu + 5;
+          const double dn2r = D[0] * nn1 + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
+          const double lim2 = -(0.001 * g0 / dT);
+          const bool t2 = dn2r > lim2;
+          const double dn2 = t2 ? lim2 : dn2r;
+          const double v2 = exp(nn1 + dn2 * dAF(nA + 2));
+          double nb[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+          const double v2b = a.ion(s, nA + 2);
+          a.ion(s, nA + 2) = 0.0;
+          const double e2 = v2b * v2;
+          double nn1b = e2;
+          const double dn2b = e2 * dAF(nA + 2);
+          if (t2) {
+            a.ion(s, nA + 2) += (dn2b * (-0.001 / dT)) / PI(s, nA + 2);
+          } else {
+            nn1b += D[0] * dn2b;
+            for (int q = 1; q < 5; ++q) nb[q] += D[q] * dn2b;
+          }
+          const double v1b = a.ion(s, nA + 1) + nn1b / v1;
+          a.ion(s, nA + 1) = 0.0;
+          const double e1 = v1b * v1;
+          nb[1] += e1;
+          const double dnb = e1 * dAF(nA + 1);
+          if (t1) {
+            a.ion(s, nA + 1) += (dnb * (-0.001 / dT)) / PI(s, nA + 1);
+          } else {
+            for (int q = 0; q < 5; ++q) nb[q + 1] += C[q] * dnb;
+          }
+          for (int j = 1; j < 6; ++j) a.ion(s, nA + 1 - j) += nb[j] / XI(s, nA + 1 - j);
+        } else {
+          const double* C = bu;
+          const double* D = bu + 5;
+          const double dn1r = C[0] * XI(s, nA) + C[1] * XI(s, nA - 1) + C[2] * XI(s, nA - 2) +
+                              C[3] * XI(s, nA - 3) + C[4] * XI(s, nA - 4);
+          const bool t1 = dn1r > -(0.001 * PI(s, nA + 1) / dT);
+          const double v1 = XI(s, nA + 1);
+          const double dn2r = D[0] * v1 + D[1] * XI(s, nA) + D[2] * XI(s, nA - 1) + D[3] * XI(s, nA - 2) +
+                              D[4] * XI(s, nA - 3);
+          const bool t2 = dn2r > -(0.001 * PI(s, nA + 2) / dT);
+          const double v2b = a.ion(s, nA + 2);
+          a.ion(s, nA + 2) = 0.0;
+          double v1b = a.ion(s, nA + 1) + v2b;
+          a.ion(s, nA + 1) = 0.0;
+          const double dn2b = v2b * dAF(nA + 2);
+          if (t2) {
+            a.ion(s, nA + 2) += dn2b * (-0.001 / dT);
+          } else {
+            v1b += D[0] * dn2b;
+            for (int q = 1; q < 5; ++q) a.ion(s, nA + 1 - q) += D[q] * dn2b;
+          }
+          a.ion(s, nA) += v1b;
+          const double dn1b = v1b * dAF(nA + 1);
+          if (t1) {
+            a.ion(s, nA + 1) += dn1b * (-0.001 / dT);
+          } else {
+            for (int q = 0; q < 5; ++q) a.ion(s, nA - q) += C[q] * dn1b;
+          }
+        }
+      }
+    }
+  }
+  // lines 466-469: Temp(nA+1:nA+2) = Temp(nA)
+  a.x(F_T, nA) += a.x(F_T, nA + 1) + a.x(F_T, nA + 2);
+  a.x(F_T, nA + 1) = 0.0;
+  a.x(F_T, nA + 2) = 0.0;
+  // lines 455-463: Vel_GD up = |Vel_GD up (nA)|
+  {
+    const double v = X(F_VU, nA);
+    const double sg = (v < 0.0) ? -1.0 : (v > 0.0 ? 1.0 : 0.0);
+    a.x(F_VU, nA) += sg * (a.x(F_VU, nA + 1) + a.x(F_VU, nA + 2));
+    a.x(F_VU, nA + 1) = 0.0;
+    a.x(F_VU, nA + 2) = 0.0;
+  }
+  // lines 420-486: species winds and hydrostatic densities
+  {
+    const double T = X(F_T, nA);
+    for (int s = 0; s < NS; ++s) {
+      const double wn = X(F_W + s, nA);
+      const double w1b = a.x(F_W + s, nA + 1), w2b = a.x(F_W + s, nA + 2);
+      a.x(F_W + s, nA + 1) = 0.0;
+      a.x(F_W + s, nA + 2) = 0.0;
+      if (photochemical(s) && wn < 0.0) {
+        a.x(F_W + s, nA) -= w1b;
+        a.x(F_W + s, nA - 1) -= w2b;
+      } else {
+        a.x(F_W + s, nA) += w1b + w2b;
+      }
+      const double ish1 = (-0.5 * (sc[SC_EG + 3] + sc[SC_EG + 2])) * c_k.mass[s] / (0.5 * (T + T) * KB);
+      const double ish2 = (-0.5 * (sc[SC_EG + 4] + sc[SC_EG + 3])) * c_k.mass[s] / (0.5 * (T + T) * KB);
+      const double lb2 = a.x(F_LNS + s, nA + 2);
+      a.x(F_LNS + s, nA + 2) = 0.0;
+      const double l1b = lb2 + a.x(F_LNS + s, nA + 1);
+      a.x(F_LNS + s, nA + 1) = 0.0;
+      const double ish2b = -sc[SC_DAF + 5] * lb2;
+      a.x(F_LNS + s, nA) += l1b;
+      const double ish1b = -sc[SC_DAF + 4] * l1b;
+      a.x(F_T, nA) += -(ish1b * ish1 + ish2b * ish2) / T;
+    }
+  }
+  // lines 420-430: horizontal winds
+  for (int f = F_VE; f <= F_VN; ++f) {
+    a.x(f, nA) += a.x(f, nA + 1) + a.x(f, nA + 2);
+    a.x(f, nA + 1) = 0.0;
+    a.x(f, nA + 2) = 0.0;
+  }
+
+  // ================= lower boundary, reversed
+  const bool msis = prm.use_msis_bcs && sc[SC_HASLBC] != 0.0;
+  // the species winds of cells 0 and -1 as the extrapolation of lines
+  // 334-344 left them (lines 382-395 may flip them afterwards)
+  double w0e[NS], wm1e[NS];
+  for (int s = 0; s < NS; ++s) {
+    const double* C0 = bl;
+    const double* C1 = bl + 5;
+    const double d0 = X(F_W + s, 1) * C0[0] + X(F_W + s, 2) * C0[1] + X(F_W + s, 3) * C0[2] +
+                      X(F_W + s, 4) * C0[3] + X(F_W + s, 5) * C0[4];
+    w0e[s] = X(F_W + s, 1) - sc[SC_DAF + 2] * d0;
+    const double d1 = w0e[s] * C1[0] + X(F_W + s, 1) * C1[1] + X(F_W + s, 2) * C1[2] + X(F_W + s, 3) * C1[3] +
+                      X(F_W + s, 4) * C1[4];
+    wm1e[s] = w0e[s] - sc[SC_DAF + 1] * d1;
+  }
+  // lines 382-395: photochemical sign flip
+  for (int s = 3; s <= 4; ++s) {
+    if (X(F_W + s, 1) > 0.0) {
+      a.x(F_W + s, 1) -= a.x(F_W + s, 0) + a.x(F_W + s, -1);
+      a.x(F_W + s, 0) = 0.0;
+      a.x(F_W + s, -1) = 0.0;
+    }
+  }
+  // lines 364-376: MSIS winds of cell -1
+  if (msis) {
+    const double* C1 = bl + 5;
+    for (int f = F_VE; f <= F_VN; ++f) {
+      const double b = a.x(f, -1);
+      a.x(f, -1) = 0.0;
+      a.x(f, 0) += b;
+      for (int q = 0; q < 5; ++q) a.x(f, q) += -sc[SC_DAF + 1] * C1[q] * b;
+    }
+  }
+  // lines 348-362: LogRho and bulk vertical wind of cells 0 and -1
+  for (int cc = 0; cc >= -1; --cc) {
+    double ms[NS], r = 0.0, mw = 0.0;
+    for (int s = 0; s < NS; ++s) {
+      ms[s] = c_k.mass[s] * exp(X(F_LNS + s, cc));
+      r = r + ms[s];
+    }
+    for (int s = 0; s < NS; ++s) mw = mw + ms[s] * (cc == 0 ? w0e[s] : wm1e[s]);
+    const double lrb = a.x(F_LRHO, cc), vub = a.x(F_VU, cc);
+    a.x(F_LRHO, cc) = 0.0;
+    a.x(F_VU, cc) = 0.0;
+    const double rb = lrb / r - vub * mw / (r * r);
+    const double mwb = vub / r;
+    for (int s = 0; s < NS; ++s) {
+      const double we = (cc == 0) ? w0e[s] : wm1e[s];
+      a.x(F_W + s, cc) += mwb * ms[s];
+      a.x(F_LNS + s, cc) += (rb + mwb * we) * ms[s];
+    }
+  }
+  // lines 304-310: ions float
+  for (int s = 0; s < NI; ++s) {
+    a.ion(s, 1) += a.ion(s, 0) + a.ion(s, -1);
+    a.ion(s, 0) = 0.0;
+    a.ion(s, -1) = 0.0;
+  }
+  // lines 205-272 and 334-344, per species
+  double l0b[NS];
+  for (int s = 0; s < NS; ++s) {
+    l0b[s] = 0.0;
+    const double* C0 = bl;
+    const double* C1 = bl + 5;
+    {  // winds: cell -1 from cell 0 (new), then cell 0 from the interior
+      const double b = a.x(F_W + s, -1);
+      a.x(F_W + s, -1) = 0.0;
+      a.x(F_W + s, 0) += b * (1.0 - sc[SC_DAF + 1] * C1[0]);
+      for (int q = 1; q < 5; ++q) a.x(F_W + s, q) += -sc[SC_DAF + 1] * C1[q] * b;
+      const double b0 = a.x(F_W + s, 0);
+      a.x(F_W + s, 0) = 0.0;
+      a.x(F_W + s, 1) += b0 * (1.0 - sc[SC_DAF + 2] * C0[0]);
+      for (int q = 1; q < 5; ++q) a.x(F_W + s, 1 + q) += -sc[SC_DAF + 2] * C0[q] * b0;
+    }
+    if (!photochemical(s)) {
+      const double b = a.x(F_LNS + s, -1);
+      a.x(F_LNS + s, -1) = 0.0;
+      if (s == 0) {
+        a.x(F_LNS + s, 0) += b;
+      } else {
+        l0b[s] = b;
+        const double ishb = b * sc[SC_DAF + 0];
+        const double mg = -0.5 * (sc[SC_EG + 0] + sc[SC_EG + 1]);
+        const double mt = 0.5 * (X(F_T, 0) + X(F_T, -1));
+        const double mm = 0.5 * (sc[SC_MMM_0] + sc[SC_MMM_M1]);
+        const double ish = mg * mm / (mt * KB);
+        const double mmb = ishb * mg / (mt * KB);
+        a.mmb[0] += 0.5 * mmb;
+        a.mmb[1] += 0.5 * mmb;
+        const double mtb = -ishb * ish / mt;
+        a.x(F_T, 0) += 0.5 * mtb;
+        a.x(F_T, -1) += 0.5 * mtb;
+      }
+    } else {
+      for (int k = 1; k >= 0; --k) {
+        const int i = -k;
+        const double* C = bl + 5 * k;
+        double d = 0.0;
+        d = X(F_LNS + s, i + 1) * C[0] + X(F_LNS + s, i + 2) * C[1] + X(F_LNS + s, i + 3) * C[2] +
+            X(F_LNS + s, i + 4) * C[3] + X(F_LNS + s, i + 5) * C[4];
+        const double up = X(F_LNS + s, i + 1);
+        const double dF = sc[SC_DAF + 2 + i];
+        double v = up - dF * d;
+        const bool flat = d <= 0.0;
+        if (flat) v = up;
+        const bool floor = (s == 4) && (v < up - 0.333);
+        const double b = a.x(F_LNS + s, i);
+        a.x(F_LNS + s, i) = 0.0;
+        a.x(F_LNS + s, i + 1) += b;
+        if (!flat && !floor) {
+          const double dbv = -dF * b;
+          for (int q = 0; q < 5; ++q) a.x(F_LNS + s, i + 1 + q) += C[q] * dbv;
+        }
+      }
+    }
+  }
+  // lines 192-196
+  for (int f : {F_T, F_VE, F_VN, F_VU}) {
+    a.x(f, 0) += a.x(f, -1);
+    a.x(f, -1) = 0.0;
+  }
+  // lines 145-148
+  a.x(F_VU, 0) = 0.0;
+  for (int s = 0; s < NS; ++s) {
+    a.x(F_W + s, 0) = 0.0;
+    a.x(F_W + s, -1) = 0.0;
+  }
+  // lines 112-143
+  a.x(F_VE, 0) = 0.0;
+  a.x(F_VN, 0) = 0.0;
+  if (msis) {
+    a.x(F_T, 0) = 0.0;
+    a.x(F_LRHO, 0) = 0.0;
+    a.x(F_LRHO, -1) = 0.0;
+    for (int s = 0; s < NS; ++s) {
+      a.x(F_LNS + s, -1) = 0.0;
+      a.x(F_LNS + s, 0) = l0b[s];
+    }
+  } else {
+    for (int s = 0; s < NS; ++s) a.x(F_LNS + s, 0) += l0b[s];
+  }
+}
+
+// ---------------------------------------------------------------- stage^T
+// Reverse of rusanov_cell at interior cell i: kb[f] is the adjoint of the
+// increment New - state of field f; contributions go to the state adjoint
+// (this cell and its neighbours), the slope adjoints, the cMax and Gamma
+// adjoints; returns the KappaEddyDiffusion adjoint of the cell.
+__device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, int i, const GitmVertParams& prm,
+                                              double dt, double eddy, double ivup, const double (&kb)[NF]) {
+  const int G = c.L.G;
+  const int nA = c.L.nAlts;
+  const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
+  const double idc = c.g(GC_IDC, i);
+  const double cmm = c.cm(i - 1), cm0 = c.cm(i), cmp = c.cm(i + 1);
+  const double fc0 = 0.5 * fmax(cmm, cm0);
+  const double fc1 = 0.5 * fmax(cm0, cmp);
+  auto sweep = [&](int f, double& grad, double& diff) {
+    const double* v = &c.col[c.xo + f * G + 1];
+    const double* d = &c.col[c.L.DL + f * (nA + 2)];
+    const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
+    const double R0 = v[i] - 0.5 * d[i] * dF0;
+    const double L1 = v[i] + 0.5 * d[i] * dF1;
+    const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
+    grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+    diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
+  };
+  double fc0b = 0.0, fc1b = 0.0;
+  double self[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) self[f] = 0.0;
+  // adjoint of one sweep: (gb, db) -> faces -> values and slopes
+  auto sweep_adj = [&](int f, double gb, double dbv) {
+    const double* v = &c.col[c.xo + f * G + 1];
+    const double* d = &c.col[c.L.DL + f * (nA + 2)];
+    const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
+    const double R0 = v[i] - 0.5 * d[i] * dF0;
+    const double L1 = v[i] + 0.5 * d[i] * dF1;
+    const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
+    const double hg = 0.5 * idc * gb;
+    const double L1b = hg - fc1 * idc * dbv, R1b = hg + fc1 * idc * dbv;
+    const double L0b = -hg + fc0 * idc * dbv, R0b = -hg - fc0 * idc * dbv;
+    fc1b += idc * (R1 - L1) * dbv;
+    fc0b += -idc * (R0 - L0) * dbv;
+    a.add(f, i - 1, L0b);
+    a.dadd(f, i - 1, 0.5 * dF0 * L0b);
+    self[f] += R0b + L1b;
+    a.dadd(f, i, -0.5 * dF0 * R0b + 0.5 * dF1 * L1b);
+    a.add(f, i + 1, R1b);
+    a.dadd(f, i + 1, -0.5 * dF1 * R1b);
+  };
+
+  // ---- forward recompute
+  const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
+  const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
+  const double LR = c.x(F_LRHO, i);
+  const double gm = c.gm(i);
+  double gT, dT, gE, dE, gN, dN, gU, dU;
+  sweep(F_T, gT, dT);
+  sweep(F_VE, gE, dE);
+  sweep(F_VN, gN, dN);
+  sweep(F_VU, gU, dU);
+  const double divv = gU + 2 * VU * invr;
+  const double itau = 1.0 / (prm.use_damping ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
+                                             : prm.vert_tau);
+  const double hz = (VN * VN + VE * VE) * invr;
+  const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
+  double wv[NS], enl[NS];
+  double sumrho = 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double gL, dL, gW, dW;
+    sweep(F_LNS + s, gL, dL);
+    sweep(F_W + s, gW, dW);
+    const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
+    const double divw = gW + 2 * Ws * invr;
+    const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
+    enl[s] = exp(nl);
+    sumrho = sumrho + c_k.mass[s] * enl[s];
+    const double km = c_k.k_over_m[s];
+    double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
+    w = w + cor;
+    w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
+    wv[s] = w;
+  }
+  double ns[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
+  const double ir = exp(-LR);
+  double glc[NS], vsol[NS], lu[NS][NS], pw[NS];
+  const double lt = log(T);
+  if (prm.use_neutral_friction) {
+    grad_log_cons(c, i, glc);
+#pragma unroll
+    for (int e = 0; e < NS; ++e) pw[e] = exp(c_k.one_minus_e[e] * lt);
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+      double rs = 0.0;
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        if (q == r) continue;
+        const double cij = c_k.kc[r][q] * ns[q] * pw[exp_index(r, q)];
+        lu[r][q] = -dt * cij;
+        rs = rs + cij;
+      }
+      lu[r][r] = 1.0 + dt * rs;
+    }
+    // LU without pivoting, multipliers kept below the diagonal
+#pragma unroll
+    for (int p = 0; p < NS; ++p)
+#pragma unroll
+      for (int r = p + 1; r < NS; ++r) {
+        const double l = lu[r][p] / lu[p][p];
+        lu[r][p] = l;
+#pragma unroll
+        for (int q = p + 1; q < NS; ++q) lu[r][q] -= l * lu[p][q];
+      }
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+      double sum = wv[r];
+#pragma unroll
+      for (int q = 0; q < r; ++q) sum -= lu[r][q] * vsol[q];
+      vsol[r] = sum;
+    }
+#pragma unroll
+    for (int r = NS - 1; r >= 0; --r) {
+      double sum = vsol[r];
+#pragma unroll
+      for (int q = r + 1; q < NS; ++q) sum -= lu[r][q] * vsol[q];
+      vsol[r] = sum / lu[r][r];
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      vsol[s] = wv[s];
+      glc[s] = 0.0;
+    }
+  }
+  double wc[NS];
+  bool inside[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double v = prm.use_neutral_friction ? vsol[s] + (-eddy * glc[s]) : vsol[s];
+    inside[s] = !(v < -prm.max_vertical_velocity) && !(v > prm.max_vertical_velocity);
+    double w = fmax(-prm.max_vertical_velocity, v);
+    wc[s] = fmin(prm.max_vertical_velocity, w);
+  }
+
+  // ---- reverse
+  double Tb = 0.0, VEb = 0.0, VNb = 0.0, VUb = 0.0, LRb = 0.0, irb = 0.0;
+  double Lb[NS], Wb[NS], nsb[NS], nlb[NS], wcb[NS];
+  // kb is the adjoint of the new values (the caller applies K = New - state)
+  // New LogRho = log(sumrho)
+  const double srb = kb[F_LRHO] / sumrho;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    nlb[s] = srb * c_k.mass[s] * enl[s];
+    Lb[s] = 0.0;
+    Wb[s] = 0.0;
+    nsb[s] = 0.0;
+  }
+  // New VU = sum_s w_s m_s ns_s / Rho; New VertVel = the clamped w
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double m = c_k.mass[s];
+    wcb[s] = kb[F_VU] * (m * ns[s] * ir) + kb[F_W + s];
+    nsb[s] += kb[F_VU] * wc[s] * m * ir;
+    irb += kb[F_VU] * wc[s] * m * ns[s];
+  }
+  double wb[NS];
+  double eddyb = 0.0;
+  if (prm.use_neutral_friction) {
+    double vb[NS], glcb[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      vb[s] = inside[s] ? wcb[s] : 0.0;
+      eddyb -= vb[s] * glc[s];
+      glcb[s] = -eddy * vb[s];
+    }
+    // wb = M^-T vb with M = L U: U^T z = vb, then L^T wb = z
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+      double sum = vb[r];
+#pragma unroll
+      for (int q = 0; q < r; ++q) sum -= lu[q][r] * wb[q];
+      wb[r] = sum / lu[r][r];
+    }
+#pragma unroll
+    for (int r = NS - 1; r >= 0; --r) {
+      double sum = wb[r];
+#pragma unroll
+      for (int q = r + 1; q < NS; ++q) sum -= lu[q][r] * wb[q];
+      wb[r] = sum;
+    }
+    // M_rq = -dt C_rq (q != r), M_rr = 1 + dt sum_q C_rq:  Cb_rq = dt wb_r (vsol_q - vsol_r)
+    double pwb[NS];
+#pragma unroll
+    for (int e = 0; e < NS; ++e) pwb[e] = 0.0;
+#pragma unroll
+    for (int r = 0; r < NS; ++r)
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        if (q == r) continue;
+        const double cb = dt * wb[r] * (vsol[q] - vsol[r]);
+        const double k = c_k.kc[r][q];
+        nsb[q] += cb * k * pw[exp_index(r, q)];
+        pwb[exp_index(r, q)] += cb * k * ns[q];
+      }
+    double ltb = 0.0;
+#pragma unroll
+    for (int e = 0; e < NS; ++e) ltb += pwb[e] * pw[e] * c_k.one_minus_e[e];
+    Tb += ltb / T;
+    // GradLogConS: 5-point mesh on log(m_s) + LogNS - LogRho
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const double mc = c.g(GC_M0 + q, i);
+      double lrb = 0.0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double v = glcb[s] * mc;
+        lrb -= v;
+        if (q == 2) Lb[s] += v; else a.add(F_LNS + s, i - 2 + q, v);
+      }
+      if (q == 2) LRb += lrb; else a.add(F_LRHO, i - 2 + q, lrb);
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) wb[s] = inside[s] ? wcb[s] : 0.0;
+  }
+  // species momentum, continuity and their sweeps
+  double gTb = 0.0, hzb = 0.0, corb = 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double gL, dL, gW, dW;
+    sweep(F_LNS + s, gL, dL);
+    sweep(F_W + s, gW, dW);
+    const double Ws = c.x(F_W + s, i);
+    const double km = c_k.k_over_m[s];
+    const double w = wb[s];
+    Wb[s] += w * (1.0 - dt * gW - itau);
+    double gWb = -dt * Ws * w;
+    hzb += dt * w;
+    Tb += -dt * gL * km * w;
+    double gLb = -dt * T * km * w;
+    gTb += -dt * km * w - dt * (prm.thermal_diff_coef[s] * km) * w;
+    const double dWb = dt * w;
+    corb += w;
+    // New LogNS = nl = Ls - dt (divw + Ws gL) + dt dL
+    const double n = nlb[s] + kb[F_LNS + s];
+    Lb[s] += n;
+    const double divwb = -dt * n;
+    Wb[s] += -dt * gL * n + 2 * invr * divwb;
+    gLb += -dt * Ws * n;
+    const double dLb = dt * n;
+    gWb += divwb;
+    sweep_adj(F_LNS + s, gLb, dLb);
+    sweep_adj(F_W + s, gWb, dWb);
+    Lb[s] += nsb[s] * ns[s];
+  }
+  LRb -= irb * ir;
+  if (prm.use_coriolis) VEb += corb * dt * c.sc(SC_CORI);
+  VNb += hzb * 2 * VN * invr;
+  VEb += hzb * 2 * VE * invr;
+  // ions: New = I - dt (IVel gI) + dt dI
+#pragma unroll
+  for (int s = 0; s < NADV; ++s) {
+    self[F_I + s] += kb[F_I + s];
+    sweep_adj(F_I + s, -dt * ivup * kb[F_I + s], dt * kb[F_I + s]);
+  }
+  // horizontal winds: New = V - dt VU gV + dt dV
+  VEb += kb[F_VE];
+  VNb += kb[F_VN];
+  VUb += -dt * gE * kb[F_VE] - dt * gN * kb[F_VN];
+  sweep_adj(F_VE, -dt * VU * kb[F_VE], dt * kb[F_VE]);
+  sweep_adj(F_VN, -dt * VU * kb[F_VN], dt * kb[F_VN]);
+  // temperature: New = T - dt (VU gT + (Gamma - 1) T divv) + dt dT
+  Tb += kb[F_T];
+  VUb += -dt * gT * kb[F_T];
+  gTb += -dt * VU * kb[F_T];
+  const double gmb = -dt * T * divv * kb[F_T];
+  Tb += -dt * (gm - 1.0) * divv * kb[F_T];
+  const double divvb = -dt * (gm - 1.0) * T * kb[F_T];
+  VUb += 2 * invr * divvb;
+  sweep_adj(F_T, gTb, dt * kb[F_T]);
+  sweep_adj(F_VU, divvb, 0.0);
+  // cMax through the dissipation coefficients
+  if (cmm >= cm0) atomicAdd(&a.cmb[i], 0.5 * fc0b); else atomicAdd(&a.cmb[i + 1], 0.5 * fc0b);
+  if (cm0 >= cmp) atomicAdd(&a.cmb[i + 1], 0.5 * fc1b); else atomicAdd(&a.cmb[i + 2], 0.5 * fc1b);
+  a.gmb[i + 1] += gmb;
+  // this cell's own contributions
+  self[F_T] += Tb;
+  self[F_VE] += VEb;
+  self[F_VN] += VNb;
+  self[F_VU] += VUb;
+  self[F_LRHO] += LRb;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    self[F_LNS + s] += Lb[s];
+    self[F_W + s] += Wb[s];
+  }
+#pragma unroll
+  for (int f = 0; f < NF; ++f) a.add(f, i, self[f]);
+  return eddyb;
+}
+
+// Adjoint of the limited slopes of cell i (interior: 4th-order form; cells 0
+// and nAlts+1: 2nd-order form) into the state adjoint.
+__device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, double beta) {
+  const int nA = c.L.nAlts;
+  const bool end = (i == 0 || i == nA + 1);
+  const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+  const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+  for (int f = 0; f < NSTENCIL; ++f) {
+    const double ob = a.db[f * (nA + 2) + i];
+    if (ob == 0.0) continue;
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    double u, d;
+    if (end) {
+      u = (v[i + 1] - v[i]) * iu;
+      d = (v[i] - v[i - 1]) * id;
+    } else {
+      u = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+      d = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
+    }
+    double ub, dbv;
+    limiter_mc_adjoint(u, d, beta, ob, ub, dbv);
+    if (ub == 0.0 && dbv == 0.0) continue;
+    if (end) {
+      a.add(f, i + 1, iu * ub);
+      a.add(f, i, -iu * ub + id * dbv);
+      a.add(f, i - 1, -id * dbv);
+    } else {
+      a.add(f, i + 2, -h2u * F2 * ub);
+      a.add(f, i + 1, h2u * F1 * ub - h2d * F2 * dbv);
+      a.add(f, i, -h2u * F1 * ub + h2d * F1 * dbv);
+      a.add(f, i - 1, h2u * F2 * ub - h2d * F1 * dbv);
+      a.add(f, i - 2, h2d * F2 * dbv);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- the kernel
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
+  extern __shared__ double sm[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  constexpr int nw = NT / 32;
+  const GitmVertParams& prm = kp.prm;
+  const double dt = kp.dt;
+  double* cta = kp.scratch + size_t(blockIdx.x) * kp.scratch_per_cta;
+  double* acc = cta + size_t(ADJ_NSTATE) * kp.nc_max * kp.per_max + tid;  // [NF] stride NT
+  double* kbs = acc + size_t(NF) * NT;                                     // [NF] stride NT
+
+  for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
+    const Tile tile = kp.tiles[tix];
+    const DevMember& M = kp.members[tile.member];
+    const GitmColumnAdjoint& B = kp.bars[tile.member];
+    const GitmColumnBatch& b = M.b;
+    const int nA = b.n_alts;
+    const int nc = tile.nc;
+    const AdjLayout A = make_adj_layout(nA);
+    const Layout& L = A.L;
+    const int G = L.G;
+    const int per = adj_state_doubles(nA);
+    const int64_t ncols = b.n_cols;
+    uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(A.stride) * nc);
+    uint32_t* sfrozen = sst + nc;
+    const int nitems = nc * nA;
+    const bool item = tid < nitems;
+    const int my_cl = item ? tid / nA : 0;
+    const int my_i = item ? tid % nA + 1 : 1;
+    int cur = 0;
+
+    auto ctx = [&](int cl) {
+      ColCtx c;
+      c.col = sm + size_t(A.stride) * cl;
+      c.L = L;
+      c.gridc = M.gridc;
+      c.gcols = M.gcols;
+      c.gc = (M.gcols == 1) ? 0 : int(tile.c0 + cl);
+      c.xo = cur ? L.X1 : L.X0;
+      c.xpo = cur ? L.XP1 : L.XP0;
+      return c;
+    };
+    auto adj = [&](int cl) {
+      ColAdj a;
+      double* col = sm + size_t(A.stride) * cl;
+      a.xb = col + L.X1;
+      a.xbp = col + L.XP1;
+      a.ob = col + L.O;
+      a.obp = col + L.OP;
+      a.db = col + A.DB;
+      a.cmb = col + A.CMB;
+      a.gmb = col + A.GMB;
+      a.tub = col + A.TUB;
+      a.mmb = col + A.MMB;
+      a.G = G;
+      a.nA = nA;
+      return a;
+    };
+    auto gidx = [&](int f, int g, int cl) -> int64_t { return (int64_t(f) * G + g) * ncols + tile.c0 + cl; };
+    auto state = [&](int s, int cl) -> double* { return cta + (size_t(s) * kp.nc_max + cl) * kp.per_max; };
+    auto save = [&](int s, int off) {
+      for (int w = tid; w < nc * per; w += NT) {
+        const int cl = w / per, r = w - cl * per;
+        state(s, cl)[r] = sm[size_t(A.stride) * cl + off + r];
+      }
+    };
+    auto load = [&](int s, int off) {
+      for (int w = tid; w < nc * per; w += NT) {
+        const int cl = w / per, r = w - cl * per;
+        sm[size_t(A.stride) * cl + off + r] = state(s, cl)[r];
+      }
+    };
+    auto boundaries = [&]() {
+      if (2 * nc <= nw) {
+        if (wid < 2 * nc) bc_column(ctx(wid >> 1), prm, lane, &sst[wid >> 1], 1 + (wid & 1));
+      } else {
+        for (int cl = wid; cl < nc; cl += nw) bc_column(ctx(cl), prm, lane, &sst[cl], 3);
+      }
+    };
+    // bc^T of every column on the state in X0 with the pre-boundary ghost
+    // values of saved state s_pre; one thread per column
+    auto boundaries_adjoint = [&](int s_pre) {
+      if (tid < nc) {
+        const double* pre = state(s_pre, tid);
+        bc_column_adjoint(ctx(tid), adj(tid), pre, pre + NF * G, prm, &sst[tid]);
+      }
+    };
+
+    if (tid < nc) {
+      sst[tid] = 0u;
+      sfrozen[tid] = 0u;
+    }
+    __syncthreads();
+
+    // ------------------------------------------------------------ gather
+    // as the forward kernel's load (IO = 0), into X0
+    if (tid < nc) {
+      ColCtx c = ctx(tid);
+      const int64_t cc = tile.c0 + tid;
+      const double cl = b.cos_lat[cc];
+      const double cent = (cl * prm.omega_body) * (cl * prm.omega_body);
+      c.sc(SC_CENT) = cent;
+      c.sc(SC_CORI) = 2 * cl * prm.omega_body;
+      const double sza = b.sza[cc], mlat = b.mlat[cc];
+      c.sc(SC_SZA) = sza;
+      c.sc(SC_MLAT) = mlat;
+      bool plasma = false;
+      if (prm.use_nighttime_ion_bcs)
+        plasma = sza > PI / 2 && ((mlat > 30.0 && mlat < 70.0) || (mlat > -60.0 && mlat < -30.0));
+      c.sc(SC_PLASMA) = plasma ? 1.0 : 0.0;
+      c.sc(SC_HASLBC) = b.lbc ? 1.0 : 0.0;
+      if (b.lbc)
+        for (int k = 0; k < 2 * GITM_LBC_NVALUES; ++k) c.sc(SC_LBC + k) = b.lbc[int64_t(k) * ncols + cc];
+      for (int j = 0; j < 20; ++j) c.sc(SC_BCC + j) = c.bcc(j);
+      const int dcell[6] = {-1, 0, 1, nA, nA + 1, nA + 2};
+      for (int j = 0; j < 6; ++j) c.sc(SC_DAF + j) = c.dAF(dcell[j]);
+      const int ecell[5] = {-1, 0, nA, nA + 1, nA + 2};
+      for (int j = 0; j < 5; ++j) c.sc(SC_EG + j) = c.g(GC_GRAV, ecell[j]) + cent * c.g(GC_R, ecell[j]);
+    }
+    for (int w = tid; w < nc * G; w += NT) {
+      const int g = w / nc, cl = w - g * nc, i = g - 1;
+      ColCtx c = ctx(cl);
+      double nd[NS], ww[NS];
+      double mn = 1.0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        nd[s] = b.ndensity_s[gidx(s, g, cl)];
+        ww[s] = b.vert_vel[gidx(s, g, cl)];
+        mn = fmin(mn, nd[s]);
+      }
+      if (!(mn > 0.0)) atomicOr(&sfrozen[cl], 1u);
+      const double temperature = b.temperature[gidx(0, g, cl)];
+      double gamma, mmm, tu, cmx = 0.0;
+      if (prm.compute_coefficients) {
+        double N = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) N = N + nd[s];
+        double gg = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
+        gamma = gg * 2.0 / N + 1;
+        double m = 0.0;
+        const double rn = 1.0 / (N + 1.0);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) m = m + c_k.mass[s] * nd[s] * rn;
+        if (m == 0) m = c_k.mass[0];
+        mmm = m;
+        tu = m * (1.0 / KB);
+        if (g >= 1 && g <= nA + 2) {
+          double mx = fabs(ww[0]);
+#pragma unroll
+          for (int s = 1; s < NS; ++s) mx = fmax(mx, fabs(ww[s]));
+          cmx = mx + sqrt(gamma * temperature);
+        }
+      } else {
+        gamma = b.gamma[gidx(0, g, cl)];
+        mmm = b.mean_major_mass[gidx(0, g, cl)];
+        tu = b.temp_unit[gidx(0, g, cl)];
+        if (g >= 1 && g <= nA + 2) cmx = b.cmax[gidx(0, g, cl)];
+      }
+      c.tu(i) = tu;
+      c.cm(i) = cmx;
+      c.gm(i) = gamma;
+      if (i == -1) c.sc(SC_MMM_M1) = mmm;
+      if (i == 0) c.sc(SC_MMM_0) = mmm;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        c.x(F_LNS + s, i) = log(nd[s]);
+        c.x(F_W + s, i) = ww[s];
+      }
+      c.x(F_T, i) = temperature * tu;
+      c.x(F_VE, i) = b.velocity[gidx(0, g, cl)];
+      c.x(F_VN, i) = b.velocity[gidx(1, g, cl)];
+      c.x(F_VU, i) = b.velocity[gidx(2, g, cl)];
+      c.x(F_LRHO, i) = log(b.rho[gidx(0, g, cl)]);
+      const bool pc = in_pcells(i, nA);
+#pragma unroll
+      for (int s = 0; s < NI; ++s) {
+        if (s >= NADV && !pc) continue;
+        const double v = b.idensity_s[gidx(s, g, cl)];
+        c.ion(s, i) = prm.use_improved_ion_advection ? v : log(v);
+      }
+    }
+    __syncthreads();
+    save(0, L.X0);
+    __syncthreads();
+    boundaries();
+    __syncthreads();
+    save(1, L.X0);
+    // Orig := X0
+    for (int w = tid; w < nc * per; w += NT) {
+      const int cl = w / per, r = w - cl * per;
+      double* col = sm + size_t(A.stride) * cl;
+      col[L.O + r] = col[L.X0 + r];
+    }
+    double eddy = 0.0, ivup = 0.0;
+    if (item) {
+      eddy = b.eddy[gidx(0, my_i + 1, my_cl)];
+      ivup = b.ivel_up[gidx(0, my_i + 1, my_cl)];
+    }
+    __syncthreads();
+
+    // ------------------------------------------------------------ forward
+    for (int k = 0; k < 4; ++k) {
+      if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
+      for (int q = tid - nitems; q < nc * 2; q += NT) {
+        if (q < 0) continue;
+        rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+      }
+      __syncthreads();
+      const int nxo = cur ? L.X0 : L.X1;
+      if (item) {
+        ColCtx c = ctx(my_cl);
+        const int i = my_i;
+        double* xn = c.col + nxo + 1;
+        auto emit = [&](int f, double kval) {
+          double& ag = acc[size_t(f) * NT];
+          const double a = (k == 0) ? kval : (k < 3) ? ag + 2.0 * kval : ag + kval;
+          ag = a;
+          const double o = c.o(f, i);
+          xn[f * G + i] = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
+        };
+        rusanov_cell(c, i, prm, dt, eddy, ivup, emit);
+      }
+      {
+        const int pr = NF * 4 + NPAS * NPC;
+        const int nxpo = cur ? L.XP0 : L.XP1;
+        for (int w = tid; w < nc * pr; w += NT) {
+          const int cl = w / pr, r = w - cl * pr;
+          double* col = sm + size_t(A.stride) * cl;
+          if (r < NF * 4) {
+            const int f = r >> 2, u = r & 3;
+            const int g = (u < 2) ? u : nA + u;
+            col[nxo + f * G + g] = col[L.O + f * G + g];
+          } else {
+            col[nxpo + r - NF * 4] = col[L.OP + r - NF * 4];
+          }
+        }
+      }
+      cur ^= 1;
+      __syncthreads();
+      boundaries();
+      __syncthreads();
+      save(2 + k, cur ? L.X1 : L.X0);
+      __syncthreads();
+    }
+    // cur == 0: X4 is in X0
+
+    // ------------------------------------------------------------ reverse
+    for (int w = tid; w < nc * A.stride; w += NT) {
+      const int cl = w / A.stride, r = w - cl * A.stride;
+      const bool z = (r >= L.X1 && r < L.X1 + per) || (r >= L.O && r < L.O + per) || (r >= A.DB);
+      if (z) sm[w] = 0.0;
+    }
+    __syncthreads();
+    // scatter^T (advance_vertical.f90:163-217 and the heating line)
+    for (int w = tid; w < nc * G; w += NT) {
+      const int g = w / nc, cl = w - g * nc, i = g - 1;
+      if (sfrozen[cl]) continue;
+      ColCtx c = ctx(cl);
+      ColAdj a = adj(cl);
+      const double tu = c.tu(i);
+      const double LR4 = c.x(F_LRHO, i), T4 = c.x(F_T, i);
+      a.x(F_LRHO, i) += B.rho[gidx(0, g, cl)] * exp(LR4);
+      a.x(F_VE, i) += B.velocity[gidx(0, g, cl)];
+      a.x(F_VN, i) += B.velocity[gidx(1, g, cl)];
+      a.x(F_VU, i) += B.velocity[gidx(2, g, cl)];
+      const double ytemp = B.temperature[gidx(0, g, cl)];
+      a.x(F_T, i) += ytemp / tu;
+      a.tub[i + 1] += -(ytemp * T4 / tu) / tu;
+      if (b.heating && i >= 1 && i <= nA && B.heating_scale)
+        atomicAdd(&a.mmb[2], ytemp * dt * b.heating[gidx(0, g, cl)]);
+      const double yN = B.ndensity ? B.ndensity[gidx(0, g, cl)] : 0.0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        a.x(F_W + s, i) += B.vert_vel[gidx(s, g, cl)];
+        const double L4 = c.x(F_LNS + s, i);
+        double v = (B.ndensity_s[gidx(s, g, cl)] + yN) * exp(L4);
+        if (B.log_ns) v += B.log_ns[gidx(s, g, cl)];
+        a.x(F_LNS + s, i) += v;
+      }
+      if (prm.use_ion_advection) {
+        const bool improved = prm.use_improved_ion_advection != 0;
+        const bool pc = in_pcells(i, nA);
+        const bool interior = (i >= 1 && i <= nA);
+        const double ye = B.idensity_s[gidx(NI, g, cl)];
+#pragma unroll
+        for (int s = 0; s < NI; ++s) {
+          if (!(s < NADV || pc)) continue;
+          const double I4 = c.ion(s, i);
+          const double v = improved ? I4 : exp(I4);
+          const bool floored = improved && interior && v < 1;
+          const double yb = B.idensity_s[gidx(s, g, cl)] + ye;
+          a.ion(s, i) += floored ? 0.0 : (improved ? yb : yb * v);
+        }
+      }
+    }
+    __syncthreads();
+    boundaries_adjoint(1);  // X4's boundaries: pre-boundary ghosts are Orig's
+    __syncthreads();
+    // combination^T of the final: X4pre = Orig + (K0 + 2K1 + 2K2 + K3) / 6
+    if (item) {
+      ColAdj a = adj(my_cl);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const double ab = (1.0 / 6.0) * a.x(f, my_i);
+        acc[size_t(f) * NT] = ab;
+        kbs[size_t(f) * NT] = ab;  // K3bar = Abar
+      }
+    }
+    __syncthreads();
+    for (int w = tid; w < nc * per; w += NT) {
+      const int cl = w / per, r = w - cl * per;
+      double* col = sm + size_t(A.stride) * cl;
+      col[L.O + r] += col[L.X1 + r];
+      col[L.X1 + r] = 0.0;
+    }
+    __syncthreads();
+
+    const double wk[4] = {1.0, 2.0, 2.0, 1.0};
+    const double ck[3] = {0.5, 0.5, 1.0};
+    for (int k = 3; k >= 0; --k) {
+      load(1 + k, L.X0);
+      for (int w = tid; w < nc * NSTENCIL * (nA + 2); w += NT) {
+        const int cl = w / (NSTENCIL * (nA + 2)), r = w - cl * (NSTENCIL * (nA + 2));
+        sm[size_t(A.stride) * cl + A.DB + r] = 0.0;
+      }
+      __syncthreads();
+      if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
+      for (int q = tid - nitems; q < nc * 2; q += NT) {
+        if (q < 0) continue;
+        rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+      }
+      __syncthreads();
+      if (item) {
+        double kb[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) kb[f] = kbs[size_t(f) * NT];
+        ColCtx c = ctx(my_cl);
+        ColAdj a = adj(my_cl);
+        const double eb = rusanov_cell_adjoint(c, a, my_i, prm, dt, eddy, ivup, kb);
+        // K = New - state: the state's own -K
+#pragma unroll
+        for (int f = 0; f < NF; ++f) a.add(f, my_i, -kb[f]);
+        if (B.eddy && !sfrozen[my_cl]) B.eddy[gidx(0, my_i + 1, my_cl)] += eb;
+      }
+      __syncthreads();
+      if (item) slopes_adjoint(ctx(my_cl), adj(my_cl), my_i, prm.beta_limiter);
+      for (int q = tid - nitems; q < nc * 2; q += NT) {
+        if (q < 0) continue;
+        slopes_adjoint(ctx(q >> 1), adj(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+      }
+      __syncthreads();
+      if (k > 0) {
+        boundaries_adjoint(1);
+        __syncthreads();
+        if (item) {
+          ColAdj a = adj(my_cl);
+#pragma unroll
+          for (int f = 0; f < NF; ++f)
+            kbs[size_t(f) * NT] = wk[k - 1] * acc[size_t(f) * NT] + ck[k - 1] * a.x(f, my_i);
+        }
+        __syncthreads();
+        for (int w = tid; w < nc * per; w += NT) {
+          const int cl = w / per, r = w - cl * per;
+          double* col = sm + size_t(A.stride) * cl;
+          col[L.O + r] += col[L.X1 + r];
+          col[L.X1 + r] = 0.0;
+        }
+        __syncthreads();
+      } else {
+        // X0 is also Orig
+        for (int w = tid; w < nc * per; w += NT) {
+          const int cl = w / per, r = w - cl * per;
+          double* col = sm + size_t(A.stride) * cl;
+          col[L.X1 + r] += col[L.O + r];
+        }
+        __syncthreads();
+        boundaries_adjoint(0);  // the first boundary pass: pre-boundary values are the gathered ones
+        __syncthreads();
+      }
+    }
+
+    // ------------------------------------------------------------ gather^T
+    for (int w = tid; w < nc * G; w += NT) {
+      const int g = w / nc, cl = w - g * nc, i = g - 1;
+      if (sfrozen[cl]) continue;
+      ColCtx c = ctx(cl);
+      ColAdj a = adj(cl);
+      double nd[NS], ww[NS], ndb[NS], wwb[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        nd[s] = b.ndensity_s[gidx(s, g, cl)];
+        ww[s] = b.vert_vel[gidx(s, g, cl)];
+        ndb[s] = a.x(F_LNS + s, i) / nd[s];
+        wwb[s] = a.x(F_W + s, i);
+      }
+      const double temperature = b.temperature[gidx(0, g, cl)];
+      const double tu = c.tu(i);
+      double tb = a.x(F_T, i) * tu;
+      double tub = a.tub[i + 1] + a.x(F_T, i) * temperature;
+      if (prm.compute_coefficients) {
+        double N = 0.0, gg = 0.0, ms = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) N = N + nd[s];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) gg = gg + nd[s] * c_k.inv_vib2[s];
+        const double gamma = gg * 2.0 / N + 1;
+        const double rn = 1.0 / (N + 1.0);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) ms = ms + c_k.mass[s] * nd[s];
+        double gammab = a.gmb[i + 1];
+        if (g >= 1 && g <= nA + 2) {
+          const double cb = a.cmb[i + 1];
+          int am = 0;
+          double mx = fabs(ww[0]);
+#pragma unroll
+          for (int s = 1; s < NS; ++s)
+            if (fabs(ww[s]) > mx) {
+              mx = fabs(ww[s]);
+              am = s;
+            }
+          wwb[am] += cb * ((ww[am] < 0.0) ? -1.0 : (ww[am] > 0.0 ? 1.0 : 0.0));
+          const double sq = sqrt(gamma * temperature);
+          gammab += cb * temperature / (2.0 * sq);
+          tb += cb * gamma / (2.0 * sq);
+        }
+        double mb = tub * (1.0 / KB);
+        if (i == -1) mb += a.mmb[0];
+        if (i == 0) mb += a.mmb[1];
+        const double rnb = mb * ms;
+        double Nb = rnb * (-rn * rn);
+        const double ggb = gammab * 2.0 / N;
+        Nb += -gammab * gg * 2.0 / (N * N);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) ndb[s] += mb * c_k.mass[s] * rn + ggb * c_k.inv_vib2[s] + Nb;
+      }
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        B.ndensity_s[gidx(s, g, cl)] = ndb[s];
+        B.vert_vel[gidx(s, g, cl)] = wwb[s];
+      }
+      B.temperature[gidx(0, g, cl)] = tb;
+      B.velocity[gidx(0, g, cl)] = a.x(F_VE, i);
+      B.velocity[gidx(1, g, cl)] = a.x(F_VN, i);
+      B.velocity[gidx(2, g, cl)] = a.x(F_VU, i);
+      B.rho[gidx(0, g, cl)] = a.x(F_LRHO, i) / b.rho[gidx(0, g, cl)];
+      if (prm.use_ion_advection) {
+        const bool improved = prm.use_improved_ion_advection != 0;
+        const bool pc = in_pcells(i, nA);
+        const double ye = B.idensity_s[gidx(NI, g, cl)];
+#pragma unroll
+        for (int s = 0; s < NI; ++s) {
+          if (s < NADV || pc) {
+            const double v = b.idensity_s[gidx(s, g, cl)];
+            B.idensity_s[gidx(s, g, cl)] = improved ? a.ion(s, i) : a.ion(s, i) / v;
+          } else {
+            B.idensity_s[gidx(s, g, cl)] += ye;  // unchanged by the step, summed into e-
+          }
+        }
+        B.idensity_s[gidx(NI, g, cl)] = 0.0;
+      }
+    }
+    if (tid < nc && !sfrozen[tid] && b.heating && B.heating_scale)
+      B.heating_scale[tile.c0 + tid] += sm[size_t(A.stride) * tid + A.MMB + 2];
+    if (tid < nc) {
+      const int64_t gcol = M.col_offset + tile.c0 + tid;
+      uint32_t wv = sst[tid];
+      if (sfrozen[tid]) wv |= GITM_ST_NEG_DENSITY;
+      if (wv) kp.status[gcol] |= wv;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace gv

@@ -489,6 +489,125 @@ __device__ __forceinline__ void grad_log_cons(const ColCtx& c, int i, double (&g
   }
 }
 
+constexpr double F1 = 0.6250000;  // Factor1, vertical_solver_rusanov.f90:739
+constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
+
+// advance_vertical_1stage (vertical_solver_rusanov.f90:387-686) at interior
+// cell i of the stage state in c, from the limited slopes in c's slope
+// buffer; emit(f, New - state) takes each field's increment.
+template <class Emit>
+__device__ __forceinline__ void rusanov_cell(const ColCtx& c, int i, const GitmVertParams& prm, double dt,
+                                             double eddy, double ivup, Emit&& emit) {
+  const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
+  const double idc = c.g(GC_IDC, i);
+  const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
+  const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
+  // calc_rusanov_alts_rusanov (:694-718) at cell i
+  auto sweep = [&](int f, double& grad, double& diff) {
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
+    const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
+    const double R0 = v[i] - 0.5 * d[i] * dF0;
+    const double L1 = v[i] + 0.5 * d[i] * dF1;
+    const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
+    grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+    diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
+  };
+  const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
+  const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
+  double gT, dT;
+  sweep(F_T, gT, dT);
+  {
+    double gE, dE, gN, dN, gU, dU;
+    sweep(F_VE, gE, dE);
+    sweep(F_VN, gN, dN);
+    sweep(F_VU, gU, dU);
+    // :660-680
+    emit(F_VE, (VE - dt * VU * gE + dt * dE) - VE);
+    emit(F_VN, (VN - dt * VU * gN + dt * dN) - VN);
+    const double divv = gU + 2 * VU * invr;
+    emit(F_T, (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T);
+  }
+  // ions 1..nIonsAdvect (:557-568)
+#pragma unroll
+  for (int s = 0; s < NADV; ++s) {
+    double gI, dI;
+    sweep(F_I + s, gI, dI);
+    const double I = c.x(F_I + s, i);
+    emit(F_I + s, (I - dt * (ivup * gI) + dt * dI) - I);
+  }
+  // species continuity and momentum (:548-617)
+  const double itau = 1.0 / (prm.use_damping
+                                 ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
+                                 : prm.vert_tau);
+  const double hz = (VN * VN + VE * VE) * invr;
+  const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
+  double wv[NS];
+  double sumrho = 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double gL, dL, gW, dW;
+    sweep(F_LNS + s, gL, dL);
+    sweep(F_W + s, gW, dW);
+    const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
+    const double divw = gW + 2 * Ws * invr;
+    const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
+    emit(F_LNS + s, nl - Ls);
+    sumrho = sumrho + c_k.mass[s] * exp(nl);
+    const double km = c_k.k_over_m[s];
+    double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
+    w = w + cor;
+    w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
+    wv[s] = w;
+  }
+  const double LR = c.x(F_LRHO, i);
+  emit(F_LRHO, log(sumrho) - LR);
+  // NS = exp(LogNS), 1 / Rho (:466-467)
+  double ns[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
+  const double ir = exp(-LR);
+  // calc_neutral_friction (calc_neutral_friction.f90:47-106)
+  if (prm.use_neutral_friction) {
+    // GradLogConS (:506-543), LogConS = log(m_s) + LogNS - LogRho
+    double glc[NS];
+    grad_log_cons(c, i, glc);
+    friction_solve(dt, ns, T, eddy, glc, wv);
+  }
+  // clamp and bulk vertical wind (:643-658)
+  double vu = 0.0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double w = fmax(-prm.max_vertical_velocity, wv[s]);
+    w = fmin(prm.max_vertical_velocity, w);
+    emit(F_W + s, w - c.x(F_W + s, i));
+    vu = vu + w * (c_k.mass[s] * ns[s] * ir);
+  }
+  emit(F_VU, vu - VU);
+}
+
+// Limited slopes of the 18 swept fields at cell i: the 4th-order form on
+// interior cells, the 2nd-order one on cells 0 and nAlts+1
+// (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772).
+__device__ __forceinline__ void rusanov_slopes_interior(const ColCtx& c, int i, double beta) {
+  const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+#pragma unroll 3
+  for (int f = 0; f < NSTENCIL; ++f) {
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+    const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
+    c.dl(f, i) = limiter_mc(up, dn, beta);
+  }
+}
+
+__device__ __forceinline__ void rusanov_slopes_end(const ColCtx& c, int i, double beta) {
+  const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+  for (int f = 0; f < NSTENCIL; ++f) {
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, beta);
+  }
+}
+
 }  // namespace gv
 
 #include "vert_ausm.cuh"
@@ -506,9 +625,6 @@ struct KParams {
   double* scratch;    // RK accumulators, NF * NT doubles per CTA (ACC_GLOBAL)
   GitmVertParams prm;
 };
-
-constexpr double F1 = 0.6250000;  // Factor1, vertical_solver_rusanov.f90:739
-constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
 
 // IO = 0: GITM arrays (advance_vertical gather/scatter);
 // IO = 1: ModVertical arrays (advance_vertical_1d_* arguments).
@@ -768,30 +884,11 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           }
         } else {
           // limited slopes of the 18 swept fields on cells 0..nAlts+1
-          // (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772)
-          if (item) {
-            ColCtx c = ctx(my_cl);
-            const int i = my_i;
-            const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
-#pragma unroll 3
-            for (int f = 0; f < NSTENCIL; ++f) {
-              const double* v = &c.col[c.xo + f * G + 1];
-              const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-              const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-              c.dl(f, i) = limiter_mc(up, dn, prm.beta_limiter);
-            }
-          }
-          // the two end slopes of each column (:764-772)
+          if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
+          // the two end slopes of each column
           for (int q = tid - nitems; q < nc * 2; q += NT) {
             if (q < 0) continue;
-            const int cl = q >> 1;
-            ColCtx c = ctx(cl);
-            const int i = (q & 1) ? nA + 1 : 0;
-            const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
-            for (int f = 0; f < NSTENCIL; ++f) {
-              const double* v = &c.col[c.xo + f * G + 1];
-              c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, prm.beta_limiter);
-            }
+            rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
           }
         }
         __syncthreads();  // @phase 2
@@ -836,92 +933,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             // advance_vertical_1stage_ausm with DtIn = Dt/2, Dt/2, Dt, Dt/2
             ausm_cell(c, i, prm, (k == 2) ? dt : 0.5 * dt, eddy, ivup, emit);
           } else {
-            const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
-            const double idc = c.g(GC_IDC, i);
-            const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
-            const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
-            // calc_rusanov_alts_rusanov (:694-718) at cell i
-            auto sweep = [&](int f, double& grad, double& diff) {
-              const double* v = &c.col[c.xo + f * G + 1];
-              const double* d = &c.col[L.DL + f * (nA + 2)];
-              const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
-              const double R0 = v[i] - 0.5 * d[i] * dF0;
-              const double L1 = v[i] + 0.5 * d[i] * dF1;
-              const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
-              grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
-              diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
-            };
-            const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
-            const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
-            double gT, dT;
-            sweep(F_T, gT, dT);
-            {
-              double gE, dE, gN, dN, gU, dU;
-              sweep(F_VE, gE, dE);
-              sweep(F_VN, gN, dN);
-              sweep(F_VU, gU, dU);
-              // :660-680
-              emit(F_VE, (VE - dt * VU * gE + dt * dE) - VE);
-              emit(F_VN, (VN - dt * VU * gN + dt * dN) - VN);
-              const double divv = gU + 2 * VU * invr;
-              emit(F_T, (T - dt * (VU * gT + (c.gm(i) - 1.0) * (T * divv)) + dt * dT) - T);
-            }
-            // ions 1..nIonsAdvect (:557-568)
-#pragma unroll
-            for (int s = 0; s < NADV; ++s) {
-              double gI, dI;
-              sweep(F_I + s, gI, dI);
-              const double I = c.x(F_I + s, i);
-              emit(F_I + s, (I - dt * (ivup * gI) + dt * dI) - I);
-            }
-            // species continuity and momentum (:548-617)
-            const double itau = 1.0 / (prm.use_damping
-                                           ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
-                                           : prm.vert_tau);
-            const double hz = (VN * VN + VE * VE) * invr;
-            const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
-            double wv[NS];
-            double sumrho = 0.0;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-              double gL, dL, gW, dW;
-              sweep(F_LNS + s, gL, dL);
-              sweep(F_W + s, gW, dW);
-              const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
-              const double divw = gW + 2 * Ws * invr;
-              const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
-              emit(F_LNS + s, nl - Ls);
-              sumrho = sumrho + c_k.mass[s] * exp(nl);
-              const double km = c_k.k_over_m[s];
-              double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
-              w = w + cor;
-              w = w - dt * (prm.thermal_diff_coef[s] * km) * gT;
-              wv[s] = w;
-            }
-            const double LR = c.x(F_LRHO, i);
-            emit(F_LRHO, log(sumrho) - LR);
-            // NS = exp(LogNS), 1 / Rho (:466-467)
-            double ns[NS];
-#pragma unroll
-            for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
-            const double ir = exp(-LR);
-            // calc_neutral_friction (calc_neutral_friction.f90:47-106)
-            if (prm.use_neutral_friction) {
-              // GradLogConS (:506-543), LogConS = log(m_s) + LogNS - LogRho
-              double glc[NS];
-              grad_log_cons(c, i, glc);
-              friction_solve(dt, ns, T, eddy, glc, wv);
-            }
-            // clamp and bulk vertical wind (:643-658)
-            double vu = 0.0;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-              double w = fmax(-prm.max_vertical_velocity, wv[s]);
-              w = fmin(prm.max_vertical_velocity, w);
-              emit(F_W + s, w - c.x(F_W + s, i));
-              vu = vu + w * (c_k.mass[s] * ns[s] * ir);
-            }
-            emit(F_VU, vu - VU);
+            rusanov_cell(c, i, prm, dt, eddy, ivup, emit);
           }
         }
         // ghost cells and passive ions of the next buffer return to Orig

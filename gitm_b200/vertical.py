@@ -37,6 +37,8 @@ STOP_MESSAGES = {
     abi.ST_LU_SINGULAR: "singular matrix in ludcmp (ludcmp.f:11-14)",
     abi.ST_NONFINITE: "NaN or Inf in the vertical solution (check_for_nans.f90)",
     abi.ST_BAD_NALTS: "nAlts outside the range of the launch",
+    abi.ST_ADJ_BRANCH: "the adjoint met the upper ion boundary's negative-density repair, which it does "
+                       "not differentiate",
 }
 
 
@@ -185,6 +187,26 @@ class Plan:
         s = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
         _check(lib().gitm_vert_plan_advance(self.handle, dt, n_steps, C.c_void_p(s)),
                self.ctx.handle, "plan_advance")
+
+    def adjoint(self, bars, dt: float, stream=None):
+        """gitm_vert_plan_adjoint: bars is one dict per member of adjoint
+        tensors named like the GitmColumnAdjoint fields (state arrays in:
+        ybar, out: xbar; eddy / heating_scale accumulate)."""
+        bars = list(bars) if isinstance(bars, (list, tuple)) else [bars]
+        arr = (abi.GitmColumnAdjoint * len(bars))()
+        torch = _torch()
+        for a, d in zip(arr, bars):
+            for name, _ in abi.GitmColumnAdjoint._fields_:
+                t = d.get(name)
+                if t is None:
+                    setattr(a, name, abi.dptr(0))
+                    continue
+                if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                    raise GitmError(f"{name}: expected a contiguous float64 CUDA tensor")
+                setattr(a, name, abi.dptr(t.data_ptr()))
+        s = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
+        _check(lib().gitm_vert_plan_adjoint(self.handle, arr, dt, C.c_void_p(s)), self.ctx.handle,
+               "plan_adjoint")
 
     def autotune(self, dt: float, n_steps: int = 1) -> abi.GitmLaunchConfig:
         c = abi.GitmLaunchConfig()

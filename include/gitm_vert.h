@@ -58,6 +58,10 @@ extern "C" {
 #define GITM_ST_LU_SINGULAR 4u  /* zero row / pivot       ludcmp.f:11-14 */
 #define GITM_ST_NONFINITE 8u    /* NaN/Inf in the result  check_for_nans.f90:4-139 */
 #define GITM_ST_BAD_NALTS 16u   /* member nAlts out of range for the launch */
+#define GITM_ST_ADJ_BRANCH 32u  /* the adjoint met a branch it does not
+                                   differentiate (negative ions next to the
+                                   top, set_vertical_bcs.Earth.f90:608-649);
+                                   that column's gradient is not valid      */
 
 /* Solver selection (ModInputs.f90:242 UseAUSMSolver). */
 #define GITM_SOLVER_RUSANOV 0
@@ -322,6 +326,40 @@ typedef struct GitmFortranState {
 int gitm_vert_advance_fortran(GitmVertCtx* ctx, const GitmFortranState* st,
                               int block_first, int block_last, double dt,
                               int on_device);
+
+/* ---- adjoint ------------------------------------------------------------
+ * No counterpart in the reference (GITM has no adjoint): the reverse-mode
+ * derivative of one step of gitm_vert_plan_advance, for gradients of
+ * rollouts.  Adjoint arrays have the layout of the GitmColumnBatch field of
+ * the same name.  On entry the state arrays hold ybar, the adjoint of the
+ * step's outputs; on return they hold xbar, the adjoint of the step's inputs
+ * (the plan's member arrays, which must hold the step's INPUT state; they are
+ * not modified).  log_ns and ndensity (may be NULL) are the adjoints of those
+ * optional outputs.  eddy and heating_scale (may be NULL) accumulate the
+ * adjoints of KappaEddyDiffusion and of the per-column heating factor.
+ * Branches (limiter cases, clamps, boundary switches, max of |w|) are
+ * differentiated on the side the step took; the electron slot of
+ * idensity_s is not an input of the step (its xbar is 0). */
+typedef struct GitmColumnAdjoint {
+  double* ndensity_s;
+  double* idensity_s;
+  double* rho;
+  double* temperature;
+  double* velocity;
+  double* vert_vel;
+  const double* log_ns;
+  const double* ndensity;
+  double* eddy;
+  double* heating_scale;
+} GitmColumnAdjoint;
+
+/* The adjoint of one step of every member of the plan (one GitmColumnAdjoint
+ * per member, device pointers).  Supported: GITM-array plans, the Rusanov
+ * solver.  Columns whose step met GITM_ST_ADJ_BRANCH set that bit in the
+ * plan's status words.  Asynchronous on `stream` (the descriptors are copied
+ * before the call returns). */
+int gitm_vert_plan_adjoint(GitmVertPlan* plan, const GitmColumnAdjoint* bars, double dt,
+                           void* stream);
 
 #ifdef __cplusplus
 }

@@ -153,6 +153,6 @@ def mesh_coefs(alt: np.ndarray):
 
 
 def abi_sizes():
-    out = (C.c_int64 * 6)()
+    out = (C.c_int64 * 7)()
     lib().oracle_abi_sizes(out)
     return list(out)

@@ -395,13 +395,14 @@ void oracle_mesh_coefs(int nAlts, const double* alt, double* out) {
 }
 
 // sizeof of the ABI structs as the C compiler lays them out.
-void oracle_abi_sizes(int64_t out[6]) {
+void oracle_abi_sizes(int64_t out[7]) {
   out[0] = sizeof(GitmVertParams);
   out[1] = sizeof(GitmColumnBatch);
   out[2] = sizeof(GitmModVerticalBatch);
   out[3] = sizeof(GitmLaunchConfig);
   out[4] = sizeof(GitmFArray);
   out[5] = sizeof(GitmFortranState);
+  out[6] = sizeof(GitmColumnAdjoint);
 }
 
 }  // extern "C"

@@ -44,7 +44,8 @@ def test_python_binding_covers_header(libpath):
 def test_struct_sizes_match_header(oracle_lib):
     sizes = oracle_lib.abi_sizes()
     py = [C.sizeof(t) for t in (abi.GitmVertParams, abi.GitmColumnBatch, abi.GitmModVerticalBatch,
-                                abi.GitmLaunchConfig, abi.GitmFArray, abi.GitmFortranState)]
+                                abi.GitmLaunchConfig, abi.GitmFArray, abi.GitmFortranState,
+                                abi.GitmColumnAdjoint)]
     assert sizes == py
 
 
