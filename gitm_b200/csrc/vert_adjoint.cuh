@@ -116,61 +116,64 @@ struct ColAdj {
 };
 
 // ---------------------------------------------------------------- boundaries^T
-// Reverse of bc_column for one column, by one thread.  c: the post-boundary
-// state; a: its adjoint, replaced by the adjoint of the pre-boundary state
-// (ghost cells the boundary overwrites get 0, ghost cells it reads before
-// overwriting get their contribution); pre / prep: the pre-boundary state's
-// cells and passive-ion cells (the values of ion ghosts the top boundary
-// reads).  Follows set_vertical_bcs.Earth.f90:8-652 as bc_column does.
+// Reverse of bc_column for one column, by a full warp with lanes over
+// species and ions as in bc_column.  part 1 = lower half, 2 = upper half,
+// 3 = both.  c: the post-boundary state; a: its adjoint, replaced by the
+// adjoint of the pre-boundary state (ghost cells the boundary overwrites get
+// 0, ghost cells it reads before overwriting get their contribution);
+// pre / prep: the pre-boundary state's cells and passive-ion cells (the
+// values of the ion ghosts the top boundary reads).  Follows
+// set_vertical_bcs.Earth.f90:8-652 as bc_column does, in reverse.  The
+// lower half writes the adjoints of cells <= 5, the upper one of cells
+// >= nAlts-4.
 __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const double* pre,
-                                         const double* prep, const GitmVertParams& prm, uint32_t* st) {
+                                         const double* prep, const GitmVertParams& prm, int lane,
+                                         uint32_t* st, int part) {
   const int nA = c.L.nAlts;
   const int G = c.L.G;
   const double* sc = c.col + c.L.SC;
+  const int s = lane;
   auto X = [&](int f, int i) -> double { return c.x(f, i); };
-  auto XI = [&](int s, int i) -> double { return c.ion(s, i); };
-  auto PI = [&](int s, int i) -> double {
-    return (s < NADV) ? pre[(F_I + s) * G + i + 1] : prep[(s - NADV) * NPC + pcell(i, nA)];
+  auto XI = [&](int q, int i) -> double { return c.ion(q, i); };
+  auto PI = [&](int q, int i) -> double {
+    return (q < NADV) ? pre[(F_I + q) * G + i + 1] : prep[(q - NADV) * NPC + pcell(i, nA)];
   };
   const double* bl = sc + SC_BCC;       // lower mesh coefficients: cell 0 then -1
   const double* bu = sc + SC_BCC + 10;  // upper: nA+1 then nA+2
   auto dAF = [&](int i) { return c.dAF(i); };
 
-  // ================= upper boundary, reversed
-  // lines 598-604: LogRho of the two top ghosts
-  for (int cc = nA + 1; cc <= nA + 2; ++cc) {
-    double ms[NS], r = 0.0;
-    for (int s = 0; s < NS; ++s) {
-      ms[s] = c_k.mass[s] * exp(X(F_LNS + s, cc));
-      r = r + ms[s];
+  if (part & 2) {
+    // lines 598-604: LogRho of the two top ghosts
+    for (int cc = nA + 1; cc <= nA + 2; ++cc) {
+      const double ms = (s < NS) ? c_k.mass[s] * exp(X(F_LNS + s, cc)) : 0.0;
+      const double r = lane_seq_sum(ms, NS);
+      const double lb = a.x(F_LRHO, cc);
+      __syncwarp();
+      if (s < NS) a.x(F_LNS + s, cc) += lb * ms / r;
+      if (s == 0) a.x(F_LRHO, cc) = 0.0;
     }
-    const double lb = a.x(F_LRHO, cc);
-    a.x(F_LRHO, cc) = 0.0;
-    for (int s = 0; s < NS; ++s) a.x(F_LNS + s, cc) += lb * ms[s] / r;
-  }
-  // lines 488-596: ions
-  {
-    const bool improved = prm.use_improved_ion_advection != 0;
-    double tp = 0.0;
-    for (int i = 1; i <= nA; ++i) tp += c.dAF(i) * (improved ? XI(0, i) : exp(XI(0, i)));
-    const bool hold = (tp / 1e16 < prm.min_tec) && (sc[SC_PLASMA] != 0.0);
-    bool neg = false;
-    if (improved)
-      for (int s = 0; s < NI; ++s)
-        for (int q = nA - 5; q <= nA + 2; ++q) {
-          const double v = (q >= nA + 1) ? PI(s, q) : XI(s, q);
-          neg = neg || (v < 0.0);
-        }
-    if (neg) {
-      atomicOr(st, GITM_ST_ADJ_BRANCH);
-    } else if (!hold) {
+    __syncwarp();
+    // lines 488-596: ions, one per lane
+    {
+      const bool improved = prm.use_improved_ion_advection != 0;
+      double tp = 0.0;
+      for (int i = 1 + lane; i <= nA; i += 32) tp += c.dAF(i) * (improved ? XI(0, i) : exp(XI(0, i)));
+      for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
+      const bool hold = (tp / 1e16 < prm.min_tec) && (sc[SC_PLASMA] != 0.0);
+      bool neg = false;
+      if (improved && s < NI)
+        for (int q = nA - 5; q <= nA + 2; ++q) neg = neg || (((q >= nA + 1) ? PI(s, q) : XI(s, q)) < 0.0);
+      const bool anyneg = __any_sync(0xffffffffu, neg);
       const double dT = dAF(nA);
-      for (int s = 0; s < NI; ++s) {
+      if (anyneg) {
+        if (lane == 0) atomicOr(st, GITM_ST_ADJ_BRANCH);
+      } else if (!hold && s < NI) {
+        const double* C = bu;
+        const double* D = bu + 5;
         if (improved) {
           double n[6];
           n[0] = log(PI(s, nA + 1));
           for (int j = 1; j < 6; ++j) n[j] = log(XI(s, nA + 1 - j));
-          const double* C = bu;
           const double dnr = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
           const double lim = -(0.001 * n[0] / dT);
           const bool t1 = dnr > lim;
@@ -178,7 +181,6 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
           const double v1 = exp(n[1] + dn * dAF(nA + 1));
           const double g0 = log(PI(s, nA + 2));
           const double nn1 = log(v1);
-          const double* D = bu + 5;
           const double dn2r = D[0] * nn1 + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
           const double lim2 = -(0.001 * g0 / dT);
           const bool t2 = dn2r > lim2;
@@ -208,8 +210,6 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
           }
           for (int j = 1; j < 6; ++j) a.ion(s, nA + 1 - j) += nb[j] / XI(s, nA + 1 - j);
         } else {
-          const double* C = bu;
-          const double* D = bu + 5;
           const double dn1r = C[0] * XI(s, nA) + C[1] * XI(s, nA - 1) + C[2] * XI(s, nA - 2) +
                               C[3] * XI(s, nA - 3) + C[4] * XI(s, nA - 4);
           const bool t1 = dn1r > -(0.001 * PI(s, nA + 1) / dT);
@@ -238,23 +238,11 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
         }
       }
     }
-  }
-  // lines 466-469: Temp(nA+1:nA+2) = Temp(nA)
-  a.x(F_T, nA) += a.x(F_T, nA + 1) + a.x(F_T, nA + 2);
-  a.x(F_T, nA + 1) = 0.0;
-  a.x(F_T, nA + 2) = 0.0;
-  // lines 455-463: Vel_GD up = |Vel_GD up (nA)|
-  {
-    const double v = X(F_VU, nA);
-    const double sg = (v < 0.0) ? -1.0 : (v > 0.0 ? 1.0 : 0.0);
-    a.x(F_VU, nA) += sg * (a.x(F_VU, nA + 1) + a.x(F_VU, nA + 2));
-    a.x(F_VU, nA + 1) = 0.0;
-    a.x(F_VU, nA + 2) = 0.0;
-  }
-  // lines 420-486: species winds and hydrostatic densities
-  {
-    const double T = X(F_T, nA);
-    for (int s = 0; s < NS; ++s) {
+    __syncwarp();
+    // lines 420-486: species winds and hydrostatic densities, one per lane
+    double tb = 0.0;
+    if (s < NS) {
+      const double T = X(F_T, nA);
       const double wn = X(F_W + s, nA);
       const double w1b = a.x(F_W + s, nA + 1), w2b = a.x(F_W + s, nA + 2);
       a.x(F_W + s, nA + 1) = 0.0;
@@ -274,156 +262,170 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
       const double ish2b = -sc[SC_DAF + 5] * lb2;
       a.x(F_LNS + s, nA) += l1b;
       const double ish1b = -sc[SC_DAF + 4] * l1b;
-      a.x(F_T, nA) += -(ish1b * ish1 + ish2b * ish2) / T;
+      tb = -(ish1b * ish1 + ish2b * ish2) / T;
     }
-  }
-  // lines 420-430: horizontal winds
-  for (int f = F_VE; f <= F_VN; ++f) {
-    a.x(f, nA) += a.x(f, nA + 1) + a.x(f, nA + 2);
-    a.x(f, nA + 1) = 0.0;
-    a.x(f, nA + 2) = 0.0;
+    tb = lane_seq_sum(tb, NS);
+    if (s == 0) {
+      // lines 466-469: Temp(nA+1:nA+2) = Temp(nA)
+      a.x(F_T, nA) += tb + a.x(F_T, nA + 1) + a.x(F_T, nA + 2);
+      a.x(F_T, nA + 1) = 0.0;
+      a.x(F_T, nA + 2) = 0.0;
+      // lines 455-463: Vel_GD up = |Vel_GD up (nA)|
+      const double v = X(F_VU, nA);
+      const double sg = (v < 0.0) ? -1.0 : (v > 0.0 ? 1.0 : 0.0);
+      a.x(F_VU, nA) += sg * (a.x(F_VU, nA + 1) + a.x(F_VU, nA + 2));
+      a.x(F_VU, nA + 1) = 0.0;
+      a.x(F_VU, nA + 2) = 0.0;
+      // lines 420-430: horizontal winds
+      for (int f = F_VE; f <= F_VN; ++f) {
+        a.x(f, nA) += a.x(f, nA + 1) + a.x(f, nA + 2);
+        a.x(f, nA + 1) = 0.0;
+        a.x(f, nA + 2) = 0.0;
+      }
+    }
+    __syncwarp();
   }
 
-  // ================= lower boundary, reversed
-  const bool msis = prm.use_msis_bcs && sc[SC_HASLBC] != 0.0;
-  // the species winds of cells 0 and -1 as the extrapolation of lines
-  // 334-344 left them (lines 382-395 may flip them afterwards)
-  double w0e[NS], wm1e[NS];
-  for (int s = 0; s < NS; ++s) {
+  if (part & 1) {
+    const bool msis = prm.use_msis_bcs && sc[SC_HASLBC] != 0.0;
     const double* C0 = bl;
     const double* C1 = bl + 5;
-    const double d0 = X(F_W + s, 1) * C0[0] + X(F_W + s, 2) * C0[1] + X(F_W + s, 3) * C0[2] +
-                      X(F_W + s, 4) * C0[3] + X(F_W + s, 5) * C0[4];
-    w0e[s] = X(F_W + s, 1) - sc[SC_DAF + 2] * d0;
-    const double d1 = w0e[s] * C1[0] + X(F_W + s, 1) * C1[1] + X(F_W + s, 2) * C1[2] + X(F_W + s, 3) * C1[3] +
-                      X(F_W + s, 4) * C1[4];
-    wm1e[s] = w0e[s] - sc[SC_DAF + 1] * d1;
-  }
-  // lines 382-395: photochemical sign flip
-  for (int s = 3; s <= 4; ++s) {
-    if (X(F_W + s, 1) > 0.0) {
-      a.x(F_W + s, 1) -= a.x(F_W + s, 0) + a.x(F_W + s, -1);
-      a.x(F_W + s, 0) = 0.0;
-      a.x(F_W + s, -1) = 0.0;
-    }
-  }
-  // lines 364-376: MSIS winds of cell -1
-  if (msis) {
-    const double* C1 = bl + 5;
-    for (int f = F_VE; f <= F_VN; ++f) {
-      const double b = a.x(f, -1);
-      a.x(f, -1) = 0.0;
-      a.x(f, 0) += b;
-      for (int q = 0; q < 5; ++q) a.x(f, q) += -sc[SC_DAF + 1] * C1[q] * b;
-    }
-  }
-  // lines 348-362: LogRho and bulk vertical wind of cells 0 and -1
-  for (int cc = 0; cc >= -1; --cc) {
-    double ms[NS], r = 0.0, mw = 0.0;
-    for (int s = 0; s < NS; ++s) {
-      ms[s] = c_k.mass[s] * exp(X(F_LNS + s, cc));
-      r = r + ms[s];
-    }
-    for (int s = 0; s < NS; ++s) mw = mw + ms[s] * (cc == 0 ? w0e[s] : wm1e[s]);
-    const double lrb = a.x(F_LRHO, cc), vub = a.x(F_VU, cc);
-    a.x(F_LRHO, cc) = 0.0;
-    a.x(F_VU, cc) = 0.0;
-    const double rb = lrb / r - vub * mw / (r * r);
-    const double mwb = vub / r;
-    for (int s = 0; s < NS; ++s) {
-      const double we = (cc == 0) ? w0e[s] : wm1e[s];
-      a.x(F_W + s, cc) += mwb * ms[s];
-      a.x(F_LNS + s, cc) += (rb + mwb * we) * ms[s];
-    }
-  }
-  // lines 304-310: ions float
-  for (int s = 0; s < NI; ++s) {
-    a.ion(s, 1) += a.ion(s, 0) + a.ion(s, -1);
-    a.ion(s, 0) = 0.0;
-    a.ion(s, -1) = 0.0;
-  }
-  // lines 205-272 and 334-344, per species
-  double l0b[NS];
-  for (int s = 0; s < NS; ++s) {
-    l0b[s] = 0.0;
-    const double* C0 = bl;
-    const double* C1 = bl + 5;
-    {  // winds: cell -1 from cell 0 (new), then cell 0 from the interior
-      const double b = a.x(F_W + s, -1);
-      a.x(F_W + s, -1) = 0.0;
-      a.x(F_W + s, 0) += b * (1.0 - sc[SC_DAF + 1] * C1[0]);
-      for (int q = 1; q < 5; ++q) a.x(F_W + s, q) += -sc[SC_DAF + 1] * C1[q] * b;
-      const double b0 = a.x(F_W + s, 0);
-      a.x(F_W + s, 0) = 0.0;
-      a.x(F_W + s, 1) += b0 * (1.0 - sc[SC_DAF + 2] * C0[0]);
-      for (int q = 1; q < 5; ++q) a.x(F_W + s, 1 + q) += -sc[SC_DAF + 2] * C0[q] * b0;
-    }
-    if (!photochemical(s)) {
-      const double b = a.x(F_LNS + s, -1);
-      a.x(F_LNS + s, -1) = 0.0;
-      if (s == 0) {
-        a.x(F_LNS + s, 0) += b;
-      } else {
-        l0b[s] = b;
-        const double ishb = b * sc[SC_DAF + 0];
-        const double mg = -0.5 * (sc[SC_EG + 0] + sc[SC_EG + 1]);
-        const double mt = 0.5 * (X(F_T, 0) + X(F_T, -1));
-        const double mm = 0.5 * (sc[SC_MMM_0] + sc[SC_MMM_M1]);
-        const double ish = mg * mm / (mt * KB);
-        const double mmb = ishb * mg / (mt * KB);
-        a.mmb[0] += 0.5 * mmb;
-        a.mmb[1] += 0.5 * mmb;
-        const double mtb = -ishb * ish / mt;
-        a.x(F_T, 0) += 0.5 * mtb;
-        a.x(F_T, -1) += 0.5 * mtb;
+    // this lane's species winds of cells 0 and -1 as the extrapolation of
+    // lines 334-344 left them (lines 382-395 may flip them afterwards)
+    double w0e = 0.0, wm1e = 0.0;
+    if (s < NS) {
+      const double d0 = X(F_W + s, 1) * C0[0] + X(F_W + s, 2) * C0[1] + X(F_W + s, 3) * C0[2] +
+                        X(F_W + s, 4) * C0[3] + X(F_W + s, 5) * C0[4];
+      w0e = X(F_W + s, 1) - sc[SC_DAF + 2] * d0;
+      const double d1 = w0e * C1[0] + X(F_W + s, 1) * C1[1] + X(F_W + s, 2) * C1[2] + X(F_W + s, 3) * C1[3] +
+                        X(F_W + s, 4) * C1[4];
+      wm1e = w0e - sc[SC_DAF + 1] * d1;
+      // lines 382-395: photochemical sign flip
+      if (photochemical(s) && X(F_W + s, 1) > 0.0) {
+        a.x(F_W + s, 1) -= a.x(F_W + s, 0) + a.x(F_W + s, -1);
+        a.x(F_W + s, 0) = 0.0;
+        a.x(F_W + s, -1) = 0.0;
       }
-    } else {
-      for (int k = 1; k >= 0; --k) {
-        const int i = -k;
-        const double* C = bl + 5 * k;
-        double d = 0.0;
-        d = X(F_LNS + s, i + 1) * C[0] + X(F_LNS + s, i + 2) * C[1] + X(F_LNS + s, i + 3) * C[2] +
-            X(F_LNS + s, i + 4) * C[3] + X(F_LNS + s, i + 5) * C[4];
-        const double up = X(F_LNS + s, i + 1);
-        const double dF = sc[SC_DAF + 2 + i];
-        double v = up - dF * d;
-        const bool flat = d <= 0.0;
-        if (flat) v = up;
-        const bool floor = (s == 4) && (v < up - 0.333);
-        const double b = a.x(F_LNS + s, i);
-        a.x(F_LNS + s, i) = 0.0;
-        a.x(F_LNS + s, i + 1) += b;
-        if (!flat && !floor) {
-          const double dbv = -dF * b;
-          for (int q = 0; q < 5; ++q) a.x(F_LNS + s, i + 1 + q) += C[q] * dbv;
+    }
+    // lines 364-376: MSIS winds of cell -1
+    if (msis && s == 0) {
+      for (int f = F_VE; f <= F_VN; ++f) {
+        const double b = a.x(f, -1);
+        a.x(f, -1) = 0.0;
+        a.x(f, 0) += b;
+        for (int q = 0; q < 5; ++q) a.x(f, q) += -sc[SC_DAF + 1] * C1[q] * b;
+      }
+    }
+    __syncwarp();
+    // lines 348-362: LogRho and bulk vertical wind of cells 0 and -1
+    for (int cc = 0; cc >= -1; --cc) {
+      const double we = (cc == 0) ? w0e : wm1e;
+      const double ms = (s < NS) ? c_k.mass[s] * exp(X(F_LNS + s, cc)) : 0.0;
+      const double r = lane_seq_sum(ms, NS);
+      const double mw = lane_seq_sum(ms * we, NS);
+      const double lrb = a.x(F_LRHO, cc), vub = a.x(F_VU, cc);
+      __syncwarp();
+      const double rb = lrb / r - vub * mw / (r * r);
+      const double mwb = vub / r;
+      if (s < NS) {
+        a.x(F_W + s, cc) += mwb * ms;
+        a.x(F_LNS + s, cc) += (rb + mwb * we) * ms;
+      }
+      if (s == 0) {
+        a.x(F_LRHO, cc) = 0.0;
+        a.x(F_VU, cc) = 0.0;
+      }
+      __syncwarp();
+    }
+    // lines 304-310: ions float
+    if (s < NI) {
+      a.ion(s, 1) += a.ion(s, 0) + a.ion(s, -1);
+      a.ion(s, 0) = 0.0;
+      a.ion(s, -1) = 0.0;
+    }
+    // lines 205-272 and 334-344, one species per lane
+    double l0b = 0.0, tb = 0.0, mb = 0.0;
+    if (s < NS) {
+      {  // winds: cell -1 from cell 0 (new), then cell 0 from the interior
+        const double b = a.x(F_W + s, -1);
+        a.x(F_W + s, -1) = 0.0;
+        a.x(F_W + s, 0) += b * (1.0 - sc[SC_DAF + 1] * C1[0]);
+        for (int q = 1; q < 5; ++q) a.x(F_W + s, q) += -sc[SC_DAF + 1] * C1[q] * b;
+        const double b0 = a.x(F_W + s, 0);
+        a.x(F_W + s, 0) = 0.0;
+        a.x(F_W + s, 1) += b0 * (1.0 - sc[SC_DAF + 2] * C0[0]);
+        for (int q = 1; q < 5; ++q) a.x(F_W + s, 1 + q) += -sc[SC_DAF + 2] * C0[q] * b0;
+      }
+      if (!photochemical(s)) {
+        const double b = a.x(F_LNS + s, -1);
+        a.x(F_LNS + s, -1) = 0.0;
+        if (s == 0) {
+          a.x(F_LNS + s, 0) += b;
+        } else {
+          l0b = b;
+          const double ishb = b * sc[SC_DAF + 0];
+          const double mg = -0.5 * (sc[SC_EG + 0] + sc[SC_EG + 1]);
+          const double mt = 0.5 * (X(F_T, 0) + X(F_T, -1));
+          const double mm = 0.5 * (sc[SC_MMM_0] + sc[SC_MMM_M1]);
+          const double ish = mg * mm / (mt * KB);
+          mb = ishb * mg / (mt * KB);
+          tb = 0.5 * (-ishb * ish / mt);
+        }
+      } else {
+        for (int k = 1; k >= 0; --k) {
+          const int i = -k;
+          const double* C = bl + 5 * k;
+          const double d = X(F_LNS + s, i + 1) * C[0] + X(F_LNS + s, i + 2) * C[1] + X(F_LNS + s, i + 3) * C[2] +
+                           X(F_LNS + s, i + 4) * C[3] + X(F_LNS + s, i + 5) * C[4];
+          const double up = X(F_LNS + s, i + 1);
+          const double dF = sc[SC_DAF + 2 + i];
+          double v = up - dF * d;
+          const bool flat = d <= 0.0;
+          if (flat) v = up;
+          const bool floor = (s == 4) && (v < up - 0.333);
+          const double b = a.x(F_LNS + s, i);
+          a.x(F_LNS + s, i) = 0.0;
+          a.x(F_LNS + s, i + 1) += b;
+          if (!flat && !floor) {
+            const double dbv = -dF * b;
+            for (int q = 0; q < 5; ++q) a.x(F_LNS + s, i + 1 + q) += C[q] * dbv;
+          }
         }
       }
     }
-  }
-  // lines 192-196
-  for (int f : {F_T, F_VE, F_VN, F_VU}) {
-    a.x(f, 0) += a.x(f, -1);
-    a.x(f, -1) = 0.0;
-  }
-  // lines 145-148
-  a.x(F_VU, 0) = 0.0;
-  for (int s = 0; s < NS; ++s) {
-    a.x(F_W + s, 0) = 0.0;
-    a.x(F_W + s, -1) = 0.0;
-  }
-  // lines 112-143
-  a.x(F_VE, 0) = 0.0;
-  a.x(F_VN, 0) = 0.0;
-  if (msis) {
-    a.x(F_T, 0) = 0.0;
-    a.x(F_LRHO, 0) = 0.0;
-    a.x(F_LRHO, -1) = 0.0;
-    for (int s = 0; s < NS; ++s) {
-      a.x(F_LNS + s, -1) = 0.0;
-      a.x(F_LNS + s, 0) = l0b[s];
+    mb = lane_seq_sum(mb, NS);
+    tb = lane_seq_sum(tb, NS);
+    if (s == 0) {
+      a.mmb[0] += 0.5 * mb;
+      a.mmb[1] += 0.5 * mb;
+      a.x(F_T, 0) += tb;
+      a.x(F_T, -1) += tb;
+      // lines 192-196
+      for (int f : {F_T, F_VE, F_VN, F_VU}) {
+        a.x(f, 0) += a.x(f, -1);
+        a.x(f, -1) = 0.0;
+      }
+      // lines 112-148
+      a.x(F_VU, 0) = 0.0;
+      a.x(F_VE, 0) = 0.0;
+      a.x(F_VN, 0) = 0.0;
+      if (msis) {
+        a.x(F_T, 0) = 0.0;
+        a.x(F_LRHO, 0) = 0.0;
+        a.x(F_LRHO, -1) = 0.0;
+      }
     }
-  } else {
-    for (int s = 0; s < NS; ++s) a.x(F_LNS + s, 0) += l0b[s];
+    if (s < NS) {
+      a.x(F_W + s, 0) = 0.0;
+      a.x(F_W + s, -1) = 0.0;
+      if (msis) {
+        a.x(F_LNS + s, -1) = 0.0;
+        a.x(F_LNS + s, 0) = l0b;
+      } else {
+        a.x(F_LNS + s, 0) += l0b;
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -848,11 +850,20 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       }
     };
     // bc^T of every column on the state in X0 with the pre-boundary ghost
-    // values of saved state s_pre; one thread per column
+    // values of saved state s_pre; a warp per column, or per column half
+    // when the halves' interior cells are disjoint
     auto boundaries_adjoint = [&](int s_pre) {
-      if (tid < nc) {
-        const double* pre = state(s_pre, tid);
-        bc_column_adjoint(ctx(tid), adj(tid), pre, pre + NF * G, prm, &sst[tid]);
+      if (2 * nc <= nw && nA >= 10) {
+        if (wid < 2 * nc) {
+          const int cl = wid >> 1;
+          const double* pre = state(s_pre, cl);
+          bc_column_adjoint(ctx(cl), adj(cl), pre, pre + NF * G, prm, lane, &sst[cl], 1 + (wid & 1));
+        }
+      } else {
+        for (int cl = wid; cl < nc; cl += nw) {
+          const double* pre = state(s_pre, cl);
+          bc_column_adjoint(ctx(cl), adj(cl), pre, pre + NF * G, prm, lane, &sst[cl], 3);
+        }
       }
     };
 
