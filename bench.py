@@ -530,9 +530,12 @@ def run_adjoint(args):
         return np.array(errs)
 
     eps = 1e-7
-    grads1 = grads_once(1)[0]
-    errs1 = fd_errors(1, grads1)
-    errs = fd_errors(args.adj_steps, grads)
+    if args.fd_directions > 0:
+        grads1 = grads_once(1)[0]
+        errs1 = fd_errors(1, grads1)
+        errs = fd_errors(args.adj_steps, grads)
+    else:
+        errs1 = errs = np.zeros(0)
     run.close()
     ctx.close()
     if rank == 0:
@@ -554,9 +557,11 @@ def run_adjoint(args):
                                "device_used_delta_bytes": int(free0 - free1)},
                "fd_check": {
                    "one_step": {"directions": int(len(errs1)), "within_1e-6": int((errs1 < 1e-6).sum()),
-                                "median_rel_err": float(np.median(errs1)), "max_rel_err": float(errs1.max())},
+                                "median_rel_err": float(np.median(errs1)) if len(errs1) else None,
+                                "max_rel_err": float(errs1.max()) if len(errs1) else None},
                    "rollout": {"steps": n, "directions": int(len(errs)), "within_1e-6": int((errs < 1e-6).sum()),
-                               "median_rel_err": float(np.median(errs)), "max_rel_err": float(errs.max())},
+                               "median_rel_err": float(np.median(errs)) if len(errs) else None,
+                               "max_rel_err": float(errs.max()) if len(errs) else None},
                    "eps_relative": eps,
                    "how": "central differences of the per-column objective, directions on one column "
                           "each, no direction filtered out, rounding floor of a few ulps of J "
