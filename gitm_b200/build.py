@@ -12,8 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgitmvert.so")
-SOURCES = ["gitm_vert.cu"]
-DEPS = ["gitm_vert.cu", "vert_kernel.cuh", "vert_ausm.cuh", "vert_adjoint.cuh", "vert_common.cuh"]
+SOURCES = ["gitm_vert.cu", "vert_adjoint.cu"]
+DEPS = ["gitm_vert.cu", "vert_adjoint.cu", "vert_kernel.cuh", "vert_ausm.cuh", "vert_adjoint.cuh", "vert_common.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

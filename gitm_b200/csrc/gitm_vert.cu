@@ -311,6 +311,7 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
   Consts k;
   fill_consts(k);
   if (cudaMemcpyToSymbol(c_k, &k, sizeof k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
+  if (adjoint_set_consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
   for (int t : kThreadChoices)
     for (int io = 0; io < 2; ++io)
       for (int solver : {GITM_SOLVER_RUSANOV, GITM_SOLVER_AUSM})
@@ -746,7 +747,7 @@ extern "C" int gitm_vert_advance_native(GitmVertCtx* ctx, const GitmColumnBatch*
 }
 
 // ------------------------------------------------------------------ adjoint
-constexpr int kAdjThreads = 128;
+constexpr int kAdjThreads = ADJ_THREADS;
 
 // Tiles, persistent grid and scratch of the adjoint kernel for the plan.
 static int adjoint_prepare(GitmVertPlan* P) {
@@ -779,7 +780,7 @@ static int adjoint_prepare(GitmVertPlan* P) {
     P->adj_ready = true;
     return GITM_OK;
   }
-  const void* fn = (const void*)vert_adjoint_kernel<kAdjThreads>;
+  const void* fn = adjoint_kernel_fn();
   CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem)));
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->adj_smem));
@@ -831,7 +832,7 @@ extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* 
   kp.scratch_per_cta = P->adj_scratch_per_cta;
   kp.prm = ctx->params;
   void* args[] = {&kp};
-  CUDA_TRY(ctx, cudaLaunchKernel((const void*)vert_adjoint_kernel<kAdjThreads>, dim3(P->adj_grid),
+  CUDA_TRY(ctx, cudaLaunchKernel(adjoint_kernel_fn(), dim3(P->adj_grid),
                                  dim3(kAdjThreads), args, P->adj_smem, st));
   return GITM_OK;
 }

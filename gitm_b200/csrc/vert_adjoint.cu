@@ -1,0 +1,20 @@
+// vert_adjoint.cu -- translation unit of the adjoint kernel.
+//
+// The adjoint kernel shares device functions with the forward step kernel
+// (rusanov_cell, bc_column, friction_solve, ...).  Compiled in the same
+// translation unit, its instantiation changes how those functions are
+// compiled into the forward kernel (a 400-byte local-memory frame and a
+// slower step), so it is built here, apart.  Without relocatable device
+// code this unit has its own copy of the constant table c_k, which the host
+// sets through adjoint_set_consts when a context is created.
+#include "vert_common.cuh"
+#include "vert_kernel.cuh"
+#include "vert_adjoint.cuh"
+
+namespace gv {
+
+const void* adjoint_kernel_fn() { return (const void*)vert_adjoint_kernel<ADJ_THREADS>; }
+
+cudaError_t adjoint_set_consts(const Consts& k) { return cudaMemcpyToSymbol(c_k, &k, sizeof k); }
+
+}  // namespace gv

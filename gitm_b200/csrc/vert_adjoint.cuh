@@ -48,7 +48,12 @@ __host__ __device__ inline size_t adj_smem_bytes(int nAlts, int nc) {
   return size_t(make_adj_layout(nAlts).stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
 }
 
-constexpr int ADJ_NSTATE = 6;  // gathered state, X0, X1, X2, X3, X4
+constexpr int ADJ_NSTATE = 6;    // gathered state, X0, X1, X2, X3, X4
+constexpr int ADJ_THREADS = 128;  // threads per CTA of the adjoint kernel
+
+// Defined in vert_adjoint.cu (the kernel's own translation unit).
+const void* adjoint_kernel_fn();
+cudaError_t adjoint_set_consts(const Consts& k);
 __host__ __device__ inline int adj_state_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
 
 struct AParams {
@@ -1001,7 +1006,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
           const double o = c.o(f, i);
           xn[f * G + i] = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
         };
-        rusanov_cell(c, i, prm, dt, eddy, ivup, emit);
+        rusanov_cell(c, i, prm, dt, eddy, ivup, 1.0 / prm.vert_tau, emit);
       }
       {
         const int pr = NF * 4 + NPAS * NPC;

@@ -32,12 +32,12 @@ constexpr int SC_QB = 59;  // dAlt_F(-1) * InvScaleHeight of the bulk gas below 
 __device__ __forceinline__ double sqr(double x) { return x * x; }
 
 // log HydroPressureS(i) - (LogNS(0) + log k + log T(0)) for species s
-__device__ __forceinline__ double hydro_q(const ColCtx& c, int s, int i) {
+__device__ __forceinline__ double hydro_q(ColCtx c, int s, int i) {
   return (i < 0) ? c.sc(SC_QB) : c_k.mass[s] * c.col[c.L.QS + i + 1];
 }
 
 // the value of AUSM slope field f at cell i
-__device__ __forceinline__ double ausm_field(const ColCtx& c, int f, int i) {
+__device__ __forceinline__ double ausm_field(ColCtx c, int f, int i) {
   if (f < AS_LPS) return c.x(F_LNS + f, i);  // LogRhoS - log m
   if (f < AS_LHPS) return c.x(F_LNS + f - AS_LPS, i) + c.col[c.L.LT + i + 1];  // LogPS - log k
   if (f < AS_W) return hydro_q(c, f - AS_LHPS, i);  // LogHPS - base
@@ -50,7 +50,7 @@ __device__ __forceinline__ double ausm_field(const ColCtx& c, int f, int i) {
 }
 
 // Phase A1: log T on every cell, and the prefix sum Q (one warp per column).
-__device__ __forceinline__ void ausm_prefix(const ColCtx& c, int lane) {
+__device__ __forceinline__ void ausm_prefix(ColCtx c, int lane) {
   const int nA = c.L.nAlts;
   double* Q = c.col + c.L.QS + 1;  // Q[i]
   double carry = 0.0;
@@ -82,7 +82,7 @@ __device__ __forceinline__ void ausm_prefix(const ColCtx& c, int lane) {
 }
 
 // Phase A2: slope of AUSM field f at cell i (0..nAlts+1).
-__device__ __forceinline__ double ausm_slope(const ColCtx& c, int f, int i, double beta) {
+__device__ __forceinline__ double ausm_slope(ColCtx c, int f, int i, double beta) {
   const int nA = c.L.nAlts;
   const double vm = ausm_field(c, f, i - 1), v0 = ausm_field(c, f, i), vp = ausm_field(c, f, i + 1);
   const bool fourth = (f >= AS_T4) && i >= 1 && i <= nA;
@@ -98,7 +98,7 @@ __device__ __forceinline__ double ausm_slope(const ColCtx& c, int f, int i, doub
 struct Faces {
   double lm, rm, lp, rp;
 };
-__device__ __forceinline__ Faces kt_faces(const ColCtx& c, int f, int i, double vm, double v0, double vp) {
+__device__ __forceinline__ Faces kt_faces(ColCtx c, int f, int i, double vm, double v0, double vp) {
   const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
   const double dfm = c.dAF(i - 1), df0 = c.dAF(i), dfp = c.dAF(i + 1);
   Faces r;
@@ -110,7 +110,7 @@ __device__ __forceinline__ Faces kt_faces(const ColCtx& c, int f, int i, double 
 }
 
 // Rusanov gradient and dissipation from the 4th-order slopes (calc_rusanov_alts_*)
-__device__ __forceinline__ void ausm_sweep(const ColCtx& c, int fslope, int ffield, int i, double fc0,
+__device__ __forceinline__ void ausm_sweep(ColCtx c, int fslope, int ffield, int i, double fc0,
                                            double fc1, double& grad, double& diff) {
   const double* v = &c.col[c.xo + ffield * c.L.G + 1];
   const double* d = &c.col[c.L.DL + fslope * (c.L.nAlts + 2)];
@@ -127,7 +127,7 @@ __device__ __forceinline__ void ausm_sweep(const ColCtx& c, int fslope, int ffie
 struct SpeciesFaces {
   Faces rho, ps, hps, w;
 };
-__device__ __forceinline__ void species_faces(const ColCtx& c, int s, int i, double logk, bool with_p,
+__device__ __forceinline__ void species_faces(ColCtx c, int s, int i, double logk, bool with_p,
                                               bool with_h, SpeciesFaces& o) {
   const double lm = c_k.log_mass[s];
   {
@@ -203,7 +203,7 @@ __device__ __forceinline__ void species_face_flux(double rl, double rr, double p
 // (densities, pressures, mass-weighted vertical wind), which set the Liou
 // sound speed; the second forms the species fluxes and applies them.
 template <class Emit>
-__device__ __forceinline__ void ausm_cell(const ColCtx& c, int i, const GitmVertParams& prm, double dtk,
+__device__ __forceinline__ void ausm_cell(ColCtx c, int i, const GitmVertParams& prm, double dtk,
                                           double eddy, double ivup, Emit&& emit) {
   const int nA = c.L.nAlts;
   (void)nA;

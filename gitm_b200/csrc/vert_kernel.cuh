@@ -473,7 +473,7 @@ __device__ __forceinline__ void friction_solve(double dt, const double (&ns)[NS]
 // GradLogConS at cell i (vertical_solver_rusanov.f90:506-543,
 // vertical_solver_ausm.f90:644-686): the 5-point mesh on
 // LogConS = log(m_s) + LogNS - LogRho of the stage state.
-__device__ __forceinline__ void grad_log_cons(const ColCtx& c, int i, double (&glc)[NS]) {
+__device__ __forceinline__ void grad_log_cons(ColCtx c, int i, double (&glc)[NS]) {
   double mc[5], lr5[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
@@ -496,8 +496,8 @@ constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
 // cell i of the stage state in c, from the limited slopes in c's slope
 // buffer; emit(f, New - state) takes each field's increment.
 template <class Emit>
-__device__ __forceinline__ void rusanov_cell(const ColCtx& c, int i, const GitmVertParams& prm, double dt,
-                                             double eddy, double ivup, Emit&& emit) {
+__device__ __forceinline__ void rusanov_cell(ColCtx c, int i, const GitmVertParams& prm, double dt,
+                                             double eddy, double ivup, double inv_vert_tau, Emit&& emit) {
   const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
   const double idc = c.g(GC_IDC, i);
   const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
@@ -537,9 +537,8 @@ __device__ __forceinline__ void rusanov_cell(const ColCtx& c, int i, const GitmV
     emit(F_I + s, (I - dt * (ivup * gI) + dt * dI) - I);
   }
   // species continuity and momentum (:548-617)
-  const double itau = 1.0 / (prm.use_damping
-                                 ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
-                                 : prm.vert_tau);
+  const double itau = prm.use_damping ? 1.0 / (15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0)
+                                      : inv_vert_tau;
   const double hz = (VN * VN + VE * VE) * invr;
   const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
   double wv[NS];
@@ -589,7 +588,7 @@ __device__ __forceinline__ void rusanov_cell(const ColCtx& c, int i, const GitmV
 // Limited slopes of the 18 swept fields at cell i: the 4th-order form on
 // interior cells, the 2nd-order one on cells 0 and nAlts+1
 // (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772).
-__device__ __forceinline__ void rusanov_slopes_interior(const ColCtx& c, int i, double beta) {
+__device__ __forceinline__ void rusanov_slopes_interior(ColCtx c, int i, double beta) {
   const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
 #pragma unroll 3
   for (int f = 0; f < NSTENCIL; ++f) {
@@ -600,7 +599,7 @@ __device__ __forceinline__ void rusanov_slopes_interior(const ColCtx& c, int i, 
   }
 }
 
-__device__ __forceinline__ void rusanov_slopes_end(const ColCtx& c, int i, double beta) {
+__device__ __forceinline__ void rusanov_slopes_end(ColCtx c, int i, double beta) {
   const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
   for (int f = 0; f < NSTENCIL; ++f) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
@@ -640,6 +639,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   const GitmVertParams& prm = kp.prm;
   const double dt = kp.dt;
   double* accg = ACC_GLOBAL ? kp.scratch + size_t(blockIdx.x) * NF * NT + tid : nullptr;
+  const double inv_vert_tau = 1.0 / prm.vert_tau;  // 1 / VertTau without damping
 
   for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
     const Tile tile = kp.tiles[tix];
@@ -904,7 +904,8 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           double* xn = c.col + nxo + 1;  // next buffer, xn[f*G + i]
           auto emit = [&](int f, double kval) {
             const int fa = ACC_GLOBAL ? 0 : f;
-            const double prev = ACC_GLOBAL ? accg[size_t(f) * NT] : accr[fa];
+            // the first stage starts the accumulator: no read of the slot
+            const double prev = (k == 0) ? 0.0 : ACC_GLOBAL ? accg[size_t(f) * NT] : accr[fa];
             const double o = c.o(f, i);
             double a, x1;
             if constexpr (SOLVER == GITM_SOLVER_AUSM) {
@@ -933,7 +934,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             // advance_vertical_1stage_ausm with DtIn = Dt/2, Dt/2, Dt, Dt/2
             ausm_cell(c, i, prm, (k == 2) ? dt : 0.5 * dt, eddy, ivup, emit);
           } else {
-            rusanov_cell(c, i, prm, dt, eddy, ivup, emit);
+            rusanov_cell(c, i, prm, dt, eddy, ivup, inv_vert_tau, emit);
           }
         }
         // ghost cells and passive ions of the next buffer return to Orig
