@@ -35,7 +35,7 @@ class StepRunner:
     """One member's arrays and a plan over them; the state arrays are
     overwritten by every call."""
 
-    def __init__(self, ctx: V.VerticalContext, member, dt: float):
+    def __init__(self, ctx: V.VerticalContext, member, dt: float, autotune: bool = True):
         self.ctx = ctx
         self.dt = float(dt)
         self.dm = V.device_member(member) if isinstance(member, synthetic.Member) else member
@@ -43,6 +43,10 @@ class StepRunner:
             self.dm.tensors["heating_scale"] = torch.ones(self.dm.n_cols, dtype=torch.float64,
                                                           device=self.dm.tensors["rho"].device)
         self.plan = V.Plan(ctx, [self.dm])
+        if autotune:
+            # one step per call: pick the fastest launch shape for that
+            # (the state is left as it was)
+            self.plan.autotune(self.dt, 1)
 
     @property
     def tensors(self):

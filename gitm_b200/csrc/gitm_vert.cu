@@ -817,9 +817,17 @@ extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* 
   if (rc) return rc;
   if (P->adj_tiles.empty()) return GITM_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUDA_TRY(ctx, cudaMemcpyAsync(P->d_bars, bars, P->n_members * sizeof(GitmColumnAdjoint),
-                                cudaMemcpyHostToDevice, st));
   AParams kp;
+  std::memset(&kp, 0, sizeof kp);
+  if (P->n_members <= ADJ_INLINE_BARS) {
+    // the descriptors travel with the launch: no copy that would wait for
+    // the stream's earlier work
+    for (int m = 0; m < P->n_members; ++m) kp.bars_inline[m] = bars[m];
+    kp.n_inline = P->n_members;
+  } else {
+    CUDA_TRY(ctx, cudaMemcpyAsync(P->d_bars, bars, P->n_members * sizeof(GitmColumnAdjoint),
+                                  cudaMemcpyHostToDevice, st));
+  }
   kp.members = P->d_members;
   kp.bars = P->d_bars;
   kp.tiles = P->d_adj_tiles;

@@ -56,9 +56,13 @@ const void* adjoint_kernel_fn();
 cudaError_t adjoint_set_consts(const Consts& k);
 __host__ __device__ inline int adj_state_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
 
+constexpr int ADJ_INLINE_BARS = 4;  // members whose descriptors travel in the kernel parameters
+
 struct AParams {
   const DevMember* members;
-  const GitmColumnAdjoint* bars;
+  const GitmColumnAdjoint* bars;      // device array (more members than fit inline)
+  GitmColumnAdjoint bars_inline[ADJ_INLINE_BARS];
+  int n_inline;                       // > 0: use bars_inline
   const Tile* tiles;
   int n_tiles;
   int nc_max;
@@ -789,7 +793,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
   for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
     const Tile tile = kp.tiles[tix];
     const DevMember& M = kp.members[tile.member];
-    const GitmColumnAdjoint& B = kp.bars[tile.member];
+    const GitmColumnAdjoint B = (kp.n_inline > 0) ? kp.bars_inline[tile.member] : kp.bars[tile.member];
     const GitmColumnBatch& b = M.b;
     const int nA = b.n_alts;
     const int nc = tile.nc;
