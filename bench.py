@@ -471,7 +471,7 @@ def run_adjoint(args):
         e2.synchronize()
         return g, e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3, float(J.detach())
 
-    grads_once(2)  # warm-up (plans, scratch)
+    grads_once(args.adj_steps)  # warm-up at full length (plans, scratch, the saved-state buffers)
     # plain forward of the same rollout: one launch per step, no checkpoints
     torch.cuda.synchronize()
     f0, f1 = ev(), ev()
@@ -551,7 +551,8 @@ def run_adjoint(args):
                "forward_plain_ms_per_step": 1e3 * t_plain / n,
                "forward_checkpointed_ms_per_step": 1e3 * t_fwd / n,
                "backward_ms_per_step": 1e3 * t_bwd / n,
-               "backward_includes": "segment recompute (forward) + one adjoint kernel per step",
+               "backward_includes": "segment recompute (the step kernel saving its stage states) + one adjoint "
+                                    "kernel per step reading them",
                "objective_value": Jv,
                "peak_memory": {"torch_allocated_bytes": int(peak_torch),
                                "device_used_delta_bytes": int(free0 - free1)},

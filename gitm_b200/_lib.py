@@ -39,7 +39,9 @@ SIGNATURES = {
     "gitm_vert_advance_native_noalloc": (C.c_int, [_P, C.POINTER(abi.GitmColumnBatch), C.c_double,
                                                    C.c_int, _P, _P]),
     "gitm_vert_advance_1d": (C.c_int, [_P, C.POINTER(abi.GitmModVerticalBatch), C.c_double, _P]),
-    "gitm_vert_plan_adjoint": (C.c_int, [_P, C.POINTER(abi.GitmColumnAdjoint), C.c_double, _P]),
+    "gitm_vert_plan_adjoint": (C.c_int, [_P, C.POINTER(abi.GitmColumnAdjoint), C.c_double, _P, _P]),
+    "gitm_vert_plan_saved_state_doubles": (C.c_int64, [_P]),
+    "gitm_vert_plan_advance_saving": (C.c_int, [_P, C.c_double, _P, _P]),
     "gitm_vert_cfl_dt": (C.c_int, [_P, C.POINTER(abi.GitmColumnBatch), C.c_int, C.c_double,
                                    C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "gitm_vert_advance_fortran": (C.c_int, [_P, C.POINTER(abi.GitmFortranState), C.c_int, C.c_int,

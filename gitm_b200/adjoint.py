@@ -11,8 +11,9 @@ sensitivity studies and data assimilation:
   differentiable torch op (``torch.autograd.Function``).
 * ``rollout(runner, state, n_steps, every, eddy, heating_scale)`` is an
   ``n_steps`` rollout that keeps only every ``every``-th state in memory and
-  recomputes the states of a segment when its adjoint runs (checkpointing),
-  each adjoint step re-running its own stages on the GPU.
+  recomputes the states of a segment when its adjoint runs (checkpointing);
+  the recompute saves each step's stage states (``step_saving``) and the
+  adjoint kernel reads them.
 * ``o_n2_objective`` is the column-weighted log(n_O / n_N2) at one altitude
   level.
 
@@ -69,9 +70,22 @@ class StepRunner:
         self.plan.advance(self.dt, 1)
         return self.state()
 
-    def vjp(self, state, ybar, eddy=None, heating_scale=None):
+    def saved_buffer(self):
+        """A device buffer for the stage states of one step."""
+        return torch.empty(self.plan.saved_state_doubles(), dtype=torch.float64,
+                           device=self.dm.tensors["rho"].device)
+
+    def step_saving(self, state, saved, eddy=None, heating_scale=None) -> dict:
+        """step() that also writes the step's stage states to `saved`."""
+        self._load(state, eddy, heating_scale)
+        self.plan.advance_saving(self.dt, saved)
+        return self.state()
+
+    def vjp(self, state, ybar, eddy=None, heating_scale=None, saved=None):
         """Adjoint of one step taken from `state`: returns (xbar, eddy_bar,
-        heating_scale_bar).  ybar: dict of output adjoints (None = zero)."""
+        heating_scale_bar).  ybar: dict of output adjoints (None = zero);
+        saved: the buffer step_saving filled for this step, or None (the
+        adjoint kernel then recomputes the stage states)."""
         self._load(state, eddy, heating_scale)
         bars = {}
         for k in STATE:
@@ -83,7 +97,7 @@ class StepRunner:
         bars["eddy"] = torch.zeros_like(self.dm.tensors["eddy"])
         hs = self.dm.tensors.get("heating_scale")
         bars["heating_scale"] = None if hs is None else torch.zeros_like(hs)
-        self.plan.adjoint([bars], self.dt)
+        self.plan.adjoint([bars], self.dt, saved=saved)
         return {k: bars[k] for k in STATE}, bars["eddy"], bars["heating_scale"]
 
     def check(self):
@@ -141,14 +155,20 @@ class _Rollout(torch.autograd.Function):
         eb = torch.zeros_like(eddy)
         hb = torch.zeros_like(hs)
         n, k = ctx.n_steps, ctx.every
+        saved = []  # one stage-state buffer per step of a segment, reused
         for seg in reversed(range(len(ctx.ckpts))):
             t0 = seg * k
             t1 = min(t0 + k, n)
+            # recompute the segment's step inputs, saving each step's stages
             states = [ctx.ckpts[seg]]
-            for _ in range(t0, t1 - 1):
-                states.append(runner.step(states[-1], eddy, hs))
-            for st in reversed(states):
-                y, e, h = runner.vjp(st, y, eddy, hs)
+            while len(saved) < t1 - t0:
+                saved.append(runner.saved_buffer())
+            for j in range(t1 - t0):
+                nxt = runner.step_saving(states[-1], saved[j], eddy, hs)
+                if j < t1 - t0 - 1:
+                    states.append(nxt)
+            for j in reversed(range(t1 - t0)):
+                y, e, h = runner.vjp(states[j], y, eddy, hs, saved=saved[j])
                 eb += e
                 if h is not None and hb.shape == h.shape:
                     hb += h

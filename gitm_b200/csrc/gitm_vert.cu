@@ -68,6 +68,10 @@ struct GitmVertPlan {
   size_t adj_scratch_per_cta = 0;
   double* d_adj_scratch = nullptr;
   GitmColumnAdjoint* d_bars = nullptr;
+  // the saving step kernel (adjoint tiles, its own persistent grid)
+  int save_grid = 0;
+  size_t save_smem = 0;
+  double* d_save_scratch = nullptr;
 };
 
 static int set_err(GitmVertCtx* ctx, int code, const char* fmt, ...) {
@@ -479,6 +483,7 @@ static void plan_free(GitmVertPlan* P) {
   if (!P) return;
   cudaFree(P->d_adj_tiles);
   cudaFree(P->d_adj_scratch);
+  cudaFree(P->d_save_scratch);
   cudaFree(P->d_bars);
   cudaFree(P->d_scratch);
   cudaFree(P->d_members);
@@ -795,18 +800,77 @@ static int adjoint_prepare(GitmVertPlan* P) {
     return set_err(ctx, GITM_ERR_NOMEM, "adjoint: cannot allocate the stage-state scratch");
   }
   CUDA_TRY(ctx, cudaMalloc(&P->d_bars, std::max(1, P->n_members) * sizeof(GitmColumnAdjoint)));
+  // the saving step kernel runs on the same tiles with the forward layout
+  const void* sfn = saving_kernel_fn();
+  CUDA_TRY(ctx, cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem)));
+  P->save_smem = 0;
+  for (const Tile& t : P->adj_tiles)
+    P->save_smem = std::max(P->save_smem, smem_bytes(P->host_members[t.member].n_alts, t.nc));
+  int sper = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, sfn, T, P->save_smem));
+  sper = std::max(sper, 1);
+  P->save_grid = int(std::min<size_t>(P->adj_tiles.size(), size_t(sper) * ctx->num_sms));
+  if (cudaMalloc(&P->d_save_scratch, size_t(P->save_grid) * NF * T * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, GITM_ERR_NOMEM, "adjoint: cannot allocate the saving step's scratch");
+  }
   P->adj_ready = true;
   return GITM_OK;
 }
 
-extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* bars, double dt, void* stream) {
+extern "C" int64_t gitm_vert_plan_saved_state_doubles(const GitmVertPlan* P) {
+  if (!P) return 0;
+  int per = 0;
+  for (const GitmColumnBatch& b : P->host_members) per = std::max(per, adj_state_doubles(b.n_alts));
+  return int64_t(ADJ_NSTATE) * P->n_cols_total * per;
+}
+
+static int adjoint_checks(GitmVertPlan* P) {
+  GitmVertCtx* ctx = P->ctx;
+  if (P->io != 0) return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint takes GITM-array plans");
+  if (P->solver != GITM_SOLVER_RUSANOV || ctx->params.solver != GITM_SOLVER_RUSANOV)
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint differentiates the Rusanov solver");
+  return GITM_OK;
+}
+
+extern "C" int gitm_vert_plan_advance_saving(GitmVertPlan* P, double dt, double* states, void* stream) {
+  if (!P) return GITM_ERR_ARG;
+  GitmVertCtx* ctx = P->ctx;
+  if (!states && P->n_cols_total > 0) return set_err(ctx, GITM_ERR_ARG, "states is NULL");
+  if (!(dt > 0.0)) return set_err(ctx, GITM_ERR_ARG, "dt must be > 0");
+  int rc = adjoint_checks(P);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  rc = adjoint_prepare(P);
+  if (rc) return rc;
+  if (P->adj_tiles.empty()) return GITM_OK;
+  KParams kp;
+  std::memset(&kp, 0, sizeof kp);
+  kp.members = P->d_members;
+  kp.tiles = P->d_adj_tiles;
+  kp.n_tiles = int(P->adj_tiles.size());
+  kp.n_steps = 1;
+  kp.dt = dt;
+  kp.status = P->d_status;
+  kp.scratch = P->d_save_scratch;
+  kp.prm = ctx->params;
+  kp.save = states;
+  kp.save_ncols = P->n_cols_total;
+  kp.save_per = P->adj_per_max;
+  void* args[] = {&kp};
+  CUDA_TRY(ctx, cudaLaunchKernel(saving_kernel_fn(), dim3(P->save_grid), dim3(ADJ_THREADS), args, P->save_smem,
+                                 static_cast<cudaStream_t>(stream)));
+  return GITM_OK;
+}
+
+extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* bars, double dt,
+                                      const double* saved_states, void* stream) {
   if (!P) return GITM_ERR_ARG;
   GitmVertCtx* ctx = P->ctx;
   if (!bars && P->n_members > 0) return set_err(ctx, GITM_ERR_ARG, "bars is NULL");
   if (!(dt > 0.0)) return set_err(ctx, GITM_ERR_ARG, "dt must be > 0");
-  if (P->io != 0) return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint takes GITM-array plans");
-  if (P->solver != GITM_SOLVER_RUSANOV || ctx->params.solver != GITM_SOLVER_RUSANOV)
-    return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint differentiates the Rusanov solver");
+  int rc0 = adjoint_checks(P);
+  if (rc0) return rc0;
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnAdjoint& a = bars[m];
     if (!a.ndensity_s || !a.idensity_s || !a.rho || !a.temperature || !a.velocity || !a.vert_vel)
@@ -839,6 +903,8 @@ extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* 
   kp.scratch = P->d_adj_scratch;
   kp.scratch_per_cta = P->adj_scratch_per_cta;
   kp.prm = ctx->params;
+  kp.saved = saved_states;
+  kp.saved_ncols = P->n_cols_total;
   void* args[] = {&kp};
   CUDA_TRY(ctx, cudaLaunchKernel(adjoint_kernel_fn(), dim3(P->adj_grid),
                                  dim3(kAdjThreads), args, P->adj_smem, st));

@@ -15,6 +15,12 @@ namespace gv {
 
 const void* adjoint_kernel_fn() { return (const void*)vert_adjoint_kernel<ADJ_THREADS>; }
 
+// The step kernel that also saves the stage states for the adjoint (GITM
+// arrays, Rusanov, 128 threads, accumulator in per-CTA scratch).
+const void* saving_kernel_fn() {
+  return (const void*)vert_step_kernel<0, ADJ_THREADS, 3, true, GITM_SOLVER_RUSANOV, true>;
+}
+
 cudaError_t adjoint_set_consts(const Consts& k) { return cudaMemcpyToSymbol(c_k, &k, sizeof k); }
 
 }  // namespace gv

@@ -53,6 +53,7 @@ constexpr int ADJ_THREADS = 128;  // threads per CTA of the adjoint kernel
 
 // Defined in vert_adjoint.cu (the kernel's own translation unit).
 const void* adjoint_kernel_fn();
+const void* saving_kernel_fn();
 cudaError_t adjoint_set_consts(const Consts& k);
 __host__ __device__ inline int adj_state_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
 
@@ -72,6 +73,11 @@ struct AParams {
   double* scratch;
   size_t scratch_per_cta;  // doubles
   GitmVertParams prm;
+  // states saved by the SAVE step kernel (gitm_vert_plan_advance_saving),
+  // state s of global column c at saved[(s * saved_ncols + c) * per_max];
+  // NULL: the kernel recomputes them
+  const double* saved;
+  int64_t saved_ncols;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -838,7 +844,12 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       return a;
     };
     auto gidx = [&](int f, int g, int cl) -> int64_t { return (int64_t(f) * G + g) * ncols + tile.c0 + cl; };
-    auto state = [&](int s, int cl) -> double* { return cta + (size_t(s) * kp.nc_max + cl) * kp.per_max; };
+    auto state = [&](int s, int cl) -> double* {
+      if (kp.saved)
+        return const_cast<double*>(kp.saved) +
+               (int64_t(s) * kp.saved_ncols + M.col_offset + tile.c0 + cl) * kp.per_max;
+      return cta + (size_t(s) * kp.nc_max + cl) * kp.per_max;
+    };
     auto save = [&](int s, int off) {
       for (int w = tid; w < nc * per; w += NT) {
         const int cl = w / per, r = w - cl * per;
@@ -971,68 +982,74 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         c.ion(s, i) = prm.use_improved_ion_advection ? v : log(v);
       }
     }
-    __syncthreads();
-    save(0, L.X0);
-    __syncthreads();
-    boundaries();
-    __syncthreads();
-    save(1, L.X0);
-    // Orig := X0
-    for (int w = tid; w < nc * per; w += NT) {
-      const int cl = w / per, r = w - cl * per;
-      double* col = sm + size_t(A.stride) * cl;
-      col[L.O + r] = col[L.X0 + r];
-    }
+    __syncthreads();  // @phase 0
     double eddy = 0.0, ivup = 0.0;
     if (item) {
       eddy = b.eddy[gidx(0, my_i + 1, my_cl)];
       ivup = b.ivel_up[gidx(0, my_i + 1, my_cl)];
     }
-    __syncthreads();
-
-    // ------------------------------------------------------------ forward
-    for (int k = 0; k < 4; ++k) {
-      if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
-      for (int q = tid - nitems; q < nc * 2; q += NT) {
-        if (q < 0) continue;
-        rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
-      }
+    if (kp.saved) {
+      // the step's states come from the saving forward: X4 into X0
+      load(5, L.X0);
       __syncthreads();
-      const int nxo = cur ? L.X0 : L.X1;
-      if (item) {
-        ColCtx c = ctx(my_cl);
-        const int i = my_i;
-        double* xn = c.col + nxo + 1;
-        auto emit = [&](int f, double kval) {
-          double& ag = acc[size_t(f) * NT];
-          const double a = (k == 0) ? kval : (k < 3) ? ag + 2.0 * kval : ag + kval;
-          ag = a;
-          const double o = c.o(f, i);
-          xn[f * G + i] = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
-        };
-        rusanov_cell(c, i, prm, dt, eddy, ivup, 1.0 / prm.vert_tau, emit);
+    } else {
+      save(0, L.X0);
+      __syncthreads();  // @phase 0
+      boundaries();
+      __syncthreads();  // @phase 1
+      save(1, L.X0);
+      // Orig := X0
+      for (int w = tid; w < nc * per; w += NT) {
+        const int cl = w / per, r = w - cl * per;
+        double* col = sm + size_t(A.stride) * cl;
+        col[L.O + r] = col[L.X0 + r];
       }
-      {
-        const int pr = NF * 4 + NPAS * NPC;
-        const int nxpo = cur ? L.XP0 : L.XP1;
-        for (int w = tid; w < nc * pr; w += NT) {
-          const int cl = w / pr, r = w - cl * pr;
-          double* col = sm + size_t(A.stride) * cl;
-          if (r < NF * 4) {
-            const int f = r >> 2, u = r & 3;
-            const int g = (u < 2) ? u : nA + u;
-            col[nxo + f * G + g] = col[L.O + f * G + g];
-          } else {
-            col[nxpo + r - NF * 4] = col[L.OP + r - NF * 4];
+      __syncthreads();  // @phase 1
+
+      // ------------------------------------------------------------ forward
+      for (int k = 0; k < 4; ++k) {
+        if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
+        for (int q = tid - nitems; q < nc * 2; q += NT) {
+          if (q < 0) continue;
+          rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+        }
+        __syncthreads();  // @phase 2
+        const int nxo = cur ? L.X0 : L.X1;
+        if (item) {
+          ColCtx c = ctx(my_cl);
+          const int i = my_i;
+          double* xn = c.col + nxo + 1;
+          auto emit = [&](int f, double kval) {
+            double& ag = acc[size_t(f) * NT];
+            const double a = (k == 0) ? kval : (k < 3) ? ag + 2.0 * kval : ag + kval;
+            ag = a;
+            const double o = c.o(f, i);
+            xn[f * G + i] = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
+          };
+          rusanov_cell(c, i, prm, dt, eddy, ivup, 1.0 / prm.vert_tau, emit);
+        }
+        {
+          const int pr = NF * 4 + NPAS * NPC;
+          const int nxpo = cur ? L.XP0 : L.XP1;
+          for (int w = tid; w < nc * pr; w += NT) {
+            const int cl = w / pr, r = w - cl * pr;
+            double* col = sm + size_t(A.stride) * cl;
+            if (r < NF * 4) {
+              const int f = r >> 2, u = r & 3;
+              const int g = (u < 2) ? u : nA + u;
+              col[nxo + f * G + g] = col[L.O + f * G + g];
+            } else {
+              col[nxpo + r - NF * 4] = col[L.OP + r - NF * 4];
+            }
           }
         }
+        cur ^= 1;
+        __syncthreads();  // @phase 3
+        boundaries();
+        __syncthreads();  // @phase 4
+        save(2 + k, cur ? L.X1 : L.X0);
+        __syncthreads();  // @phase 1
       }
-      cur ^= 1;
-      __syncthreads();
-      boundaries();
-      __syncthreads();
-      save(2 + k, cur ? L.X1 : L.X0);
-      __syncthreads();
     }
     // cur == 0: X4 is in X0
 
@@ -1042,7 +1059,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       const bool z = (r >= L.X1 && r < L.X1 + per) || (r >= L.O && r < L.O + per) || (r >= A.DB);
       if (z) sm[w] = 0.0;
     }
-    __syncthreads();
+    __syncthreads();  // @phase 0
     // scatter^T (advance_vertical.f90:163-217 and the heating line)
     for (int w = tid; w < nc * G; w += NT) {
       const int g = w / nc, cl = w - g * nc, i = g - 1;
@@ -1085,9 +1102,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         }
       }
     }
-    __syncthreads();
+    __syncthreads();  // @phase 5
     boundaries_adjoint(1);  // X4's boundaries: pre-boundary ghosts are Orig's
-    __syncthreads();
+    __syncthreads();  // @phase 6
     // combination^T of the final: X4pre = Orig + (K0 + 2K1 + 2K2 + K3) / 6
     if (item) {
       ColAdj a = adj(my_cl);
@@ -1098,14 +1115,14 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         kbs[size_t(f) * NT] = ab;  // K3bar = Abar
       }
     }
-    __syncthreads();
+    __syncthreads();  // @phase 7
     for (int w = tid; w < nc * per; w += NT) {
       const int cl = w / per, r = w - cl * per;
       double* col = sm + size_t(A.stride) * cl;
       col[L.O + r] += col[L.X1 + r];
       col[L.X1 + r] = 0.0;
     }
-    __syncthreads();
+    __syncthreads();  // @phase 7
 
     const double wk[4] = {1.0, 2.0, 2.0, 1.0};
     const double ck[3] = {0.5, 0.5, 1.0};
@@ -1115,13 +1132,13 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         const int cl = w / (NSTENCIL * (nA + 2)), r = w - cl * (NSTENCIL * (nA + 2));
         sm[size_t(A.stride) * cl + A.DB + r] = 0.0;
       }
-      __syncthreads();
+      __syncthreads();  // @phase 8
       if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
       for (int q = tid - nitems; q < nc * 2; q += NT) {
         if (q < 0) continue;
         rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
       }
-      __syncthreads();
+      __syncthreads();  // @phase 8
       if (item) {
         double kb[NF];
 #pragma unroll
@@ -1134,30 +1151,30 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         for (int f = 0; f < NF; ++f) a.add(f, my_i, -kb[f]);
         if (B.eddy && !sfrozen[my_cl]) B.eddy[gidx(0, my_i + 1, my_cl)] += eb;
       }
-      __syncthreads();
+      __syncthreads();  // @phase 9
       if (item) slopes_adjoint(ctx(my_cl), adj(my_cl), my_i, prm.beta_limiter);
       for (int q = tid - nitems; q < nc * 2; q += NT) {
         if (q < 0) continue;
         slopes_adjoint(ctx(q >> 1), adj(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
       }
-      __syncthreads();
+      __syncthreads();  // @phase 10
       if (k > 0) {
         boundaries_adjoint(1);
-        __syncthreads();
+        __syncthreads();  // @phase 6
         if (item) {
           ColAdj a = adj(my_cl);
 #pragma unroll
           for (int f = 0; f < NF; ++f)
             kbs[size_t(f) * NT] = wk[k - 1] * acc[size_t(f) * NT] + ck[k - 1] * a.x(f, my_i);
         }
-        __syncthreads();
+        __syncthreads();  // @phase 7
         for (int w = tid; w < nc * per; w += NT) {
           const int cl = w / per, r = w - cl * per;
           double* col = sm + size_t(A.stride) * cl;
           col[L.O + r] += col[L.X1 + r];
           col[L.X1 + r] = 0.0;
         }
-        __syncthreads();
+        __syncthreads();  // @phase 7
       } else {
         // X0 is also Orig
         for (int w = tid; w < nc * per; w += NT) {
@@ -1165,9 +1182,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
           double* col = sm + size_t(A.stride) * cl;
           col[L.X1 + r] += col[L.O + r];
         }
-        __syncthreads();
+        __syncthreads();  // @phase 7
         boundaries_adjoint(0);  // the first boundary pass: pre-boundary values are the gathered ones
-        __syncthreads();
+        __syncthreads();  // @phase 6
       }
     }
 
@@ -1259,7 +1276,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       if (sfrozen[tid]) wv |= GITM_ST_NEG_DENSITY;
       if (wv) kp.status[gcol] |= wv;
     }
-    __syncthreads();
+    __syncthreads();  // @phase 11
   }
 }
 

@@ -623,6 +623,12 @@ struct KParams {
   uint32_t* status;   // one word per column (member col_offset + column)
   double* scratch;    // RK accumulators, NF * NT doubles per CTA (ACC_GLOBAL)
   GitmVertParams prm;
+  // SAVE kernels (one step per launch): the gathered state and the
+  // post-boundary stage states X0..X4 of every column, state s of global
+  // column c at save[(s * save_ncols + c) * save_per], for the adjoint
+  double* save;
+  int64_t save_ncols;
+  int save_per;
 };
 
 // IO = 0: GITM arrays (advance_vertical gather/scatter);
@@ -630,7 +636,7 @@ struct KParams {
 // ACC_GLOBAL: the RK accumulator of each item lives in a per-CTA slot of
 // kp.scratch (coalesced, L2-resident under a persistent grid) instead of
 // registers, which lets small CTAs share an SM.
-template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER>
+template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER, bool SAVE = false>
 __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
@@ -670,6 +676,19 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
     };
     auto gidx = [&](int f, int g, int cl) -> int64_t {
       return (int64_t(f) * G + g) * ncols + tile.c0 + cl;
+    };
+    // SAVE: copies the current stage buffer (state and passive cells) of
+    // every column of the tile to saved state s
+    auto save_state = [&](int s) {
+      if constexpr (SAVE) {
+        const int per = NF * G + NPAS * NPC;
+        const int xo = cur ? L.X1 : L.X0;
+        for (int w = tid; w < nc * per; w += NT) {
+          const int cl = w / per, r = w - cl * per;
+          const int64_t gcol = M.col_offset + tile.c0 + cl;
+          kp.save[(int64_t(s) * kp.save_ncols + gcol) * kp.save_per + r] = sm[size_t(L.stride) * cl + xo + r];
+        }
+      }
     };
     // set_vertical_bcs for every column of the tile: the lower and upper
     // halves of a column go to different warps when there are enough
@@ -828,6 +847,10 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
       }
     }
     __syncthreads();  // @phase 0
+    if constexpr (SAVE) {
+      save_state(0);
+      __syncthreads();  // the boundary pass rewrites what was just saved
+    }
 
     // per-item constants for the step
     double eddy = 0.0, ivup = 0.0;
@@ -846,6 +869,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
       // ---------------------------------------------------- first BC pass
       boundaries();
       __syncthreads();  // @phase 1
+      save_state(1);
       // Orig = state (vertical_solver_rusanov.f90:95-100); read first in
       // phase B, after the barrier that ends phase A
       {
@@ -959,6 +983,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         // set_vertical_bcs on the updated state (:166,236,306,368)
         boundaries();
         __syncthreads();  // @phase 1
+        save_state(2 + k);
       }
 
       // ---------------------------------------------------- store / reload

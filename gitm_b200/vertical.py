@@ -188,10 +188,26 @@ class Plan:
         _check(lib().gitm_vert_plan_advance(self.handle, dt, n_steps, C.c_void_p(s)),
                self.ctx.handle, "plan_advance")
 
-    def adjoint(self, bars, dt: float, stream=None):
+    def saved_state_doubles(self) -> int:
+        """Doubles of the buffer advance_saving fills."""
+        return int(lib().gitm_vert_plan_saved_state_doubles(self.handle))
+
+    def advance_saving(self, dt: float, states, stream=None):
+        """gitm_vert_plan_advance_saving: one step that also saves its stage
+        states (a float64 CUDA tensor of saved_state_doubles() elements)."""
+        torch = _torch()
+        if not (states.is_cuda and states.dtype == torch.float64 and states.is_contiguous()
+                and states.numel() >= self.saved_state_doubles()):
+            raise GitmError("states: expected a contiguous float64 CUDA tensor of saved_state_doubles() elements")
+        s = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
+        _check(lib().gitm_vert_plan_advance_saving(self.handle, dt, C.c_void_p(states.data_ptr()), C.c_void_p(s)),
+               self.ctx.handle, "plan_advance_saving")
+
+    def adjoint(self, bars, dt: float, saved=None, stream=None):
         """gitm_vert_plan_adjoint: bars is one dict per member of adjoint
         tensors named like the GitmColumnAdjoint fields (state arrays in:
-        ybar, out: xbar; eddy / heating_scale accumulate)."""
+        ybar, out: xbar; eddy / heating_scale accumulate).  saved: the
+        buffer advance_saving filled for this step, or None."""
         bars = list(bars) if isinstance(bars, (list, tuple)) else [bars]
         arr = (abi.GitmColumnAdjoint * len(bars))()
         torch = _torch()
@@ -205,7 +221,8 @@ class Plan:
                     raise GitmError(f"{name}: expected a contiguous float64 CUDA tensor")
                 setattr(a, name, abi.dptr(t.data_ptr()))
         s = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
-        _check(lib().gitm_vert_plan_adjoint(self.handle, arr, dt, C.c_void_p(s)), self.ctx.handle,
+        sp = 0 if saved is None else saved.data_ptr()
+        _check(lib().gitm_vert_plan_adjoint(self.handle, arr, dt, C.c_void_p(sp), C.c_void_p(s)), self.ctx.handle,
                "plan_adjoint")
 
     def autotune(self, dt: float, n_steps: int = 1) -> abi.GitmLaunchConfig:

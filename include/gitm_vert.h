@@ -356,10 +356,22 @@ typedef struct GitmColumnAdjoint {
 /* The adjoint of one step of every member of the plan (one GitmColumnAdjoint
  * per member, device pointers).  Supported: GITM-array plans, the Rusanov
  * solver.  Columns whose step met GITM_ST_ADJ_BRANCH set that bit in the
- * plan's status words.  Asynchronous on `stream` (the descriptors are copied
- * before the call returns). */
+ * plan's status words.  saved_states: the states gitm_vert_plan_advance_saving
+ * wrote for this step, or NULL to recompute them inside the adjoint kernel.
+ * Asynchronous on `stream` (the descriptors are read before the call
+ * returns). */
 int gitm_vert_plan_adjoint(GitmVertPlan* plan, const GitmColumnAdjoint* bars, double dt,
-                           void* stream);
+                           const double* saved_states, void* stream);
+
+/* Doubles of the device buffer one gitm_vert_plan_advance_saving call fills
+ * (the gathered state and the five post-boundary stage states of every
+ * column). */
+int64_t gitm_vert_plan_saved_state_doubles(const GitmVertPlan* plan);
+
+/* One step of gitm_vert_plan_advance (GITM-array plan, Rusanov) that also
+ * writes the step's stage states to `states` (device, the size above) for a
+ * later gitm_vert_plan_adjoint of the same step.  Asynchronous on `stream`. */
+int gitm_vert_plan_advance_saving(GitmVertPlan* plan, double dt, double* states, void* stream);
 
 #ifdef __cplusplus
 }
