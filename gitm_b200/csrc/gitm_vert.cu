@@ -35,9 +35,16 @@ struct GitmVertCtx {
   size_t arena_bytes = 0;
   double* d_scalar = nullptr;  // one double for reductions
   cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
+  // the host-pointer path keeps its plan while the calls' chunking, staging
+  // arena and altitude grids stay the same
+  GitmVertPlan* host_plan = nullptr;
+  std::vector<uint64_t> host_plan_key;
+  std::vector<cudaEvent_t> events;  // chunk hand-offs between the host path's streams
 };
 
 static int arena_reserve(GitmVertCtx* ctx, size_t bytes);
+struct GitmVertPlan;
+static void plan_free(GitmVertPlan* P);
 
 struct GitmVertPlan {
   GitmVertCtx* ctx = nullptr;
@@ -328,6 +335,8 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
 int gitm_vert_destroy(GitmVertCtx* ctx) {
   if (!ctx) return GITM_OK;
   cudaSetDevice(ctx->device);
+  plan_free(ctx->host_plan);
+  for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   cudaFree(ctx->arena);
   cudaFree(ctx->d_scalar);
   for (cudaStream_t& st : ctx->streams)
@@ -987,7 +996,8 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
   for (cudaStream_t& st : ctx->streams)
     if (!st) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   const GitmVertParams& prm = ctx->params;
-  // chunking: about 8 chunks per member, at least 2048 columns each
+  // chunking: about 16 chunks per member, at least 1024 columns each (the
+  // copies of one chunk overlap the step of another)
   struct Chunk { int m; int64_t c0, n; size_t off; };
   std::vector<Chunk> chunks;
   size_t total = 0;
@@ -996,7 +1006,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     if (rc) return rc;
     const GitmColumnBatch& b = members[m];
     const int G = b.n_alts + 4;
-    const int64_t per = std::max<int64_t>(2048, (b.n_cols + 7) / 8);
+    const int64_t per = std::max<int64_t>(1024, (b.n_cols + 15) / 16);
     for (int64_t c0 = 0; c0 < b.n_cols; c0 += per) {
       Chunk ch{m, c0, std::min(per, b.n_cols - c0), total};
       size_t rows = 0;
@@ -1053,25 +1063,76 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
       CUDA_TRY(ctx, cudaMemcpy2D(const_cast<double*>(dst[q]), w, src[q] + chunks[j].c0, hp, w, G,
                                  cudaMemcpyHostToDevice));
   }
+  // the plan of the previous call serves again when nothing it was built
+  // from changed: the staging arena, the solver, the chunks and the shared
+  // altitude grids (compared by value); per-column grids build a new plan
+  std::vector<uint64_t> key;
+  bool cacheable = true;
+  auto put = [&](double v) { uint64_t u; std::memcpy(&u, &v, 8); key.push_back(u); };
+  key.push_back(uint64_t(reinterpret_cast<uintptr_t>(ctx->arena)));
+  key.push_back(uint64_t(prm.solver));
+  for (const Chunk& ch : chunks) {
+    const GitmColumnBatch& b = members[ch.m];
+    key.push_back(uint64_t(ch.m));
+    key.push_back(uint64_t(ch.c0));
+    key.push_back(uint64_t(ch.n));
+    key.push_back(uint64_t(b.n_alts));
+    if (b.grid_per_column) cacheable = false;
+  }
+  for (int m = 0; m < n_members && cacheable; ++m) {
+    const GitmColumnBatch& b = members[m];
+    uint64_t present = 0, bit = 1;  // which arrays the call passes (they set the arena layout)
+    for (const ArraySpec& a : kArrays) { if (b.*(a.field)) present |= bit; bit <<= 1; }
+    for (const ConstSpec& a : kInputs) { if (b.*(a.field)) present |= bit; bit <<= 1; }
+    key.push_back(present);
+    key.push_back(uint64_t(b.n_cols));
+    for (const double* g : {b.altitude, b.gravity, b.dalt_c, b.inv_r})
+      for (int i = 0; i < b.n_alts + 4; ++i) put(g[i]);
+  }
   GitmVertPlan* P = nullptr;
-  // plan_create checks that state arrays are device pointers: they are
-  rc = gitm_vert_plan_create(ctx, dm.data(), int(dm.size()), &P);
-  if (rc) return rc;
+  if (cacheable && ctx->host_plan && key == ctx->host_plan_key) {
+    P = ctx->host_plan;
+  } else {
+    plan_free(ctx->host_plan);
+    ctx->host_plan = nullptr;
+    ctx->host_plan_key.clear();
+    // plan_create checks that state arrays are device pointers: they are
+    rc = gitm_vert_plan_create(ctx, dm.data(), int(dm.size()), &P);
+    if (rc) return rc;
+    // 128 threads with the accumulator in scratch, persistent grid
+    GitmLaunchConfig cfg{128, 0, 1, 0};
+    rc = gitm_vert_plan_set_config(P, &cfg);
+    if (rc) { plan_free(P); return rc; }
+    if (cacheable) {
+      ctx->host_plan = P;
+      ctx->host_plan_key = key;
+    }
+  }
   // tile ranges per chunk (tiles are ordered by member)
   std::vector<int> t0(chunks.size() + 1, int(P->tiles.size()));
   for (int t = int(P->tiles.size()) - 1; t >= 0; --t) t0[P->tiles[t].member] = t;
   for (int j = int(chunks.size()) - 1; j >= 0; --j)
     if (t0[j] > t0[j + 1]) t0[j] = t0[j + 1];
   const void* fn = kernel_for(0, P->solver, P->cfg.threads);
+  // one stream per role: copies in (streams[0]), steps (streams[1]), copies
+  // out (streams[2]); a chunk's step waits for its copies in and its copies
+  // out wait for its step, so each copy engine streams without waiting for
+  // the other direction
+  cudaStream_t s_in = ctx->streams[0], s_k = ctx->streams[1], s_out = ctx->streams[2];
+  while (ctx->events.size() < 2 * chunks.size()) {
+    cudaEvent_t e;
+    CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->events.push_back(e);
+  }
   for (size_t j = 0; j < chunks.size() && !rc; ++j) {
     const Chunk& ch = chunks[j];
     const GitmColumnBatch& b = members[ch.m];
     const GitmColumnBatch& d = dm[j];
     const int G = b.n_alts + 4;
-    cudaStream_t st = ctx->streams[j % 3];
     const size_t hp = size_t(b.n_cols) * sizeof(double), w = size_t(ch.n) * sizeof(double);
+    cudaEvent_t e_in = ctx->events[2 * j], e_k = ctx->events[2 * j + 1];
     auto h2d = [&](double* dst, const double* src, int64_t rows) -> int {
-      CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, w, src + ch.c0, hp, w, rows, cudaMemcpyHostToDevice, st));
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, w, src + ch.c0, hp, w, rows, cudaMemcpyHostToDevice, s_in));
       return GITM_OK;
     };
     for (const ArraySpec& a : kArrays) {
@@ -1089,8 +1150,11 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
       if ((rc = h2d(const_cast<double*>(d.*(a.field)), b.*(a.field), rows_of(a.rows_per_cell, G)))) break;
     }
     if (rc) break;
+    CUDA_TRY(ctx, cudaEventRecord(e_in, s_in));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, e_in, 0));
     const int spl = std::max(1, P->cfg.steps_per_launch);
     KParams kp;
+    std::memset(&kp, 0, sizeof kp);
     kp.members = P->d_members;
     kp.tiles = P->d_tiles + t0[j];
     kp.n_tiles = t0[j + 1] - t0[j];
@@ -1098,32 +1162,32 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     kp.status = P->d_status;
     kp.scratch = P->d_scratch;
     kp.prm = prm;
-    // chunks run on three streams at once: each gets a third of the
-    // persistent grid's scratch slots
-    const int third = std::max(1, P->grid / 3);
-    if (P->d_scratch) kp.scratch = P->d_scratch + size_t(j % 3) * third * NF * P->cfg.threads;
-    const int cgrid = P->d_scratch ? std::min(kp.n_tiles, third) : kp.n_tiles;
+    const int cgrid = P->d_scratch ? std::min(kp.n_tiles, P->grid) : kp.n_tiles;
     for (int done = 0; done < n_steps && kp.n_tiles > 0; done += spl) {
       kp.n_steps = std::min(spl, n_steps - done);
       void* args[] = {&kp};
-      cudaError_t e = cudaLaunchKernel(fn, dim3(cgrid), dim3(P->cfg.threads), args, P->smem, st);
+      cudaError_t e = cudaLaunchKernel(fn, dim3(cgrid), dim3(P->cfg.threads), args, P->smem, s_k);
       if (e != cudaSuccess) { rc = set_err(ctx, GITM_ERR_CUDA, "launch: %s", cudaGetErrorString(e)); break; }
     }
+    if (rc) break;
+    CUDA_TRY(ctx, cudaEventRecord(e_k, s_k));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(s_out, e_k, 0));
     for (const ArraySpec& a : kArrays) {
       if (rc || !a.out || !(b.*(a.field))) continue;
       if (!prm.compute_coefficients && (a.field == &GitmColumnBatch::gamma || a.field == &GitmColumnBatch::mean_major_mass ||
                                         a.field == &GitmColumnBatch::temp_unit || a.field == &GitmColumnBatch::cmax))
         continue;
       cudaError_t e = cudaMemcpy2DAsync(b.*(a.field) + ch.c0, hp, d.*(a.field), w, w,
-                                        rows_of(a.rows_per_cell, G), cudaMemcpyDeviceToHost, st);
+                                        rows_of(a.rows_per_cell, G), cudaMemcpyDeviceToHost, s_out);
       if (e != cudaSuccess) rc = set_err(ctx, GITM_ERR_CUDA, "copy back: %s", cudaGetErrorString(e));
     }
   }
   for (cudaStream_t st : ctx->streams) cudaStreamSynchronize(st);
   uint32_t sto = 0;
   int64_t nbad = 0;
-  if (!rc) rc = gitm_vert_plan_status(P, &sto, &nbad, 0);
-  plan_free(P);
+  const int rcs = gitm_vert_plan_status(P, &sto, &nbad, 1);
+  if (!rc) rc = rcs;
+  if (P != ctx->host_plan) plan_free(P);
   if (!rc && sto) rc = set_err(ctx, GITM_ERR_COLUMN, "%lld columns reported status 0x%x", (long long)nbad, sto);
   (void)is_pinned_host;
   return rc;
