@@ -30,9 +30,10 @@ module ModGitmVertC
   type, bind(C) :: GitmVertParams
      integer(c_int32_t) :: solver, use_neutral_friction, use_coriolis, &
           use_ion_advection, use_improved_ion_advection, use_nighttime_ion_bcs, &
-          use_damping, use_msis_bcs, compute_coefficients, reserved0
+          use_damping, use_msis_bcs, compute_coefficients, compute_eddy
      real(c_double) :: beta_limiter, max_vertical_velocity, min_tec, omega_body, vert_tau
      real(c_double) :: thermal_diff_coef(6)
+     real(c_double) :: eddy_coef, eddy_pressure0, eddy_pressure1
   end type GitmVertParams
 
   type, bind(C) :: GitmFArray
@@ -133,6 +134,7 @@ contains
     p%use_damping = merge(1, 0, UseDamping)
     p%use_msis_bcs = 0   ! the MSIS lower boundary is passed as a table (lbc) by the native API
     p%compute_coefficients = 0   ! calc_pressure / calc_timestep / calc_rates ran on the host
+    p%compute_eddy = 0           ! calc_sources (KappaEddyDiffusion) runs on the host
     p%beta_limiter = BetaLimiter
     p%max_vertical_velocity = MaximumVerticalVelocity
     p%min_tec = MinTEC

@@ -45,13 +45,16 @@ class GitmVertParams(C.Structure):
         ("use_damping", C.c_int32),
         ("use_msis_bcs", C.c_int32),
         ("compute_coefficients", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("compute_eddy", C.c_int32),
         ("beta_limiter", C.c_double),
         ("max_vertical_velocity", C.c_double),
         ("min_tec", C.c_double),
         ("omega_body", C.c_double),
         ("vert_tau", C.c_double),
         ("thermal_diff_coef", C.c_double * NSPECIES),
+        ("eddy_coef", C.c_double),
+        ("eddy_pressure0", C.c_double),
+        ("eddy_pressure1", C.c_double),
     ]
 
 
@@ -77,6 +80,10 @@ def default_params(**overrides) -> GitmVertParams:
     for i in range(NSPECIES):
         p.thermal_diff_coef[i] = 0.0
     p.thermal_diff_coef[5] = -0.38
+    p.compute_eddy = 0
+    p.eddy_coef = 50.0        # EddyDiffusionCoef, ModInputs.f90:302
+    p.eddy_pressure0 = 0.01   # EddyDiffusionPressure0 (Pa), :303
+    p.eddy_pressure1 = 0.005  # EddyDiffusionPressure1 (Pa), :304
     for k, v in overrides.items():
         if k == "thermal_diff_coef":
             for i in range(NSPECIES):

@@ -285,6 +285,10 @@ void gitm_vert_default_params(GitmVertParams* p) {
   p->omega_body = 2.0 * 3.141592653589793 / (24.0 * 3600.0);
   p->vert_tau = 1.0e9;
   p->thermal_diff_coef[5] = -0.38;
+  p->compute_eddy = 0;
+  p->eddy_coef = 50.0;
+  p->eddy_pressure0 = 0.01;
+  p->eddy_pressure1 = 0.005;
 }
 
 static int check_params(GitmVertCtx* ctx, const GitmVertParams* p) {
@@ -293,6 +297,8 @@ static int check_params(GitmVertCtx* ctx, const GitmVertParams* p) {
     return set_err(ctx, GITM_ERR_ARG, "unknown solver %d", p->solver);
   if (!(p->beta_limiter >= 1.0 && p->beta_limiter <= 2.0))
     return set_err(ctx, GITM_ERR_ARG, "beta_limiter %g outside [1, 2]", p->beta_limiter);
+  if (p->compute_eddy && !(p->eddy_pressure0 > p->eddy_pressure1))
+    return set_err(ctx, GITM_ERR_ARG, "compute_eddy needs eddy_pressure0 > eddy_pressure1");
   return GITM_OK;
 }
 
@@ -666,7 +672,7 @@ static int snapshot(GitmVertPlan* P, std::vector<std::pair<double*, double*>>& b
                                              {b.rho, 1}, {b.temperature, 1}, {b.velocity, 3},
                                              {b.vert_vel, NS}, {b.log_ns, NS}, {b.ndensity, 1},
                                              {b.gamma, 1}, {b.mean_major_mass, 1},
-                                             {b.temp_unit, 1}, {b.cmax, 1}};
+                                             {b.temp_unit, 1}, {b.cmax, 1}, {b.eddy, 1}};
       for (auto& f : fs) {
         if (!f.p) continue;
         double* cp = nullptr;
@@ -686,7 +692,7 @@ static int snapshot(GitmVertPlan* P, std::vector<std::pair<double*, double*>>& b
                                            {b.rho, 1}, {b.temperature, 1}, {b.velocity, 3},
                                            {b.vert_vel, NS}, {b.log_ns, NS}, {b.ndensity, 1},
                                            {b.gamma, 1}, {b.mean_major_mass, 1},
-                                           {b.temp_unit, 1}, {b.cmax, 1}};
+                                           {b.temp_unit, 1}, {b.cmax, 1}, {b.eddy, 1}};
     for (auto& f : fs) {
       if (!f.p) continue;
       CUDA_TRY(ctx, cudaMemcpy(f.p, bk[idx].second, cells * f.k * sizeof(double), cudaMemcpyDeviceToDevice));
@@ -839,6 +845,8 @@ static int adjoint_checks(GitmVertPlan* P) {
   if (P->io != 0) return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint takes GITM-array plans");
   if (P->solver != GITM_SOLVER_RUSANOV || ctx->params.solver != GITM_SOLVER_RUSANOV)
     return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint differentiates the Rusanov solver");
+  if (ctx->params.compute_eddy)
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "the adjoint takes the eddy coefficient as an input: compute_eddy must be 0");
   return GITM_OK;
 }
 
@@ -967,14 +975,14 @@ const ArraySpec kArrays[] = {
     {&GitmColumnBatch::mean_major_mass, 1, true, true},
     {&GitmColumnBatch::temp_unit, 1, true, true},
     {&GitmColumnBatch::cmax, 1, true, true},
+    {&GitmColumnBatch::eddy, 1, true, true},  // copied back when compute_eddy = 1
 };
 struct ConstSpec {
   const double* GitmColumnBatch::* field;
   int rows_per_cell;  // as above
 };
 const ConstSpec kInputs[] = {
-    {&GitmColumnBatch::ivel_up, 1},   {&GitmColumnBatch::eddy, 1},
-    {&GitmColumnBatch::cos_lat, 0},   {&GitmColumnBatch::sza, 0},
+    {&GitmColumnBatch::ivel_up, 1},   {&GitmColumnBatch::cos_lat, 0},   {&GitmColumnBatch::sza, 0},
     {&GitmColumnBatch::mlat, 0},      {&GitmColumnBatch::lbc, -1},
     {&GitmColumnBatch::altitude, 1},  {&GitmColumnBatch::gravity, 1},
     {&GitmColumnBatch::dalt_c, 1},    {&GitmColumnBatch::inv_r, 1},
@@ -1177,6 +1185,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
       if (!prm.compute_coefficients && (a.field == &GitmColumnBatch::gamma || a.field == &GitmColumnBatch::mean_major_mass ||
                                         a.field == &GitmColumnBatch::temp_unit || a.field == &GitmColumnBatch::cmax))
         continue;
+      if (!prm.compute_eddy && a.field == &GitmColumnBatch::eddy) continue;
       cudaError_t e = cudaMemcpy2DAsync(b.*(a.field) + ch.c0, hp, d.*(a.field), w, w,
                                         rows_of(a.rows_per_cell, G), cudaMemcpyDeviceToHost, s_out);
       if (e != cudaSuccess) rc = set_err(ctx, GITM_ERR_CUDA, "copy back: %s", cudaGetErrorString(e));
@@ -1206,6 +1215,8 @@ extern "C" int gitm_vert_advance_1d(GitmVertCtx* ctx, const GitmModVerticalBatch
   for (const void* p : req)
     if (!p || !is_device_ptr(p)) return set_err(ctx, GITM_ERR_ARG, "ModVertical arrays must be non-NULL device pointers");
   if (ctx->params.use_msis_bcs && !v.lbc) return set_err(ctx, GITM_ERR_ARG, "use_msis_bcs=1 needs the lbc table");
+  if (ctx->params.compute_eddy)
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "compute_eddy applies to the GITM-array form");
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   GitmVertPlan* P = new GitmVertPlan();
   P->ctx = ctx;
@@ -1440,6 +1451,7 @@ extern "C" int gitm_vert_advance_fortran(GitmVertCtx* ctx, const GitmFortranStat
 
   GitmVertParams saved = ctx->params;
   ctx->params.compute_coefficients = 0;
+  ctx->params.compute_eddy = 0;  // calc_sources runs on the host
   GitmColumnBatch b;
   std::memset(&b, 0, sizeof b);
   b.n_alts = nA;

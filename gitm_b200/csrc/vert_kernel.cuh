@@ -1031,6 +1031,20 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         }
         const bool improved = prm.use_improved_ion_advection != 0;
         const bool interior = (i >= 1 && i <= nA);
+        if (prm.compute_eddy && interior && sfrozen[cl] == 0u) {
+          // calc_eddy_diffusion_coefficient (Earth.f90:376-411) on Pressure =
+          // Temperature * Rho (calc_pressure.f90:23) of the state this step
+          // started from (Orig, with this step's TempUnit): the coefficient
+          // the next step reads (calc_sources.f90:26 runs after the vertical
+          // advance)
+          const double pr = (c.o(F_T, i) / c.tu(i)) * exp(c.o(F_LRHO, i));
+          double kz = 0.0;
+          if (pr > prm.eddy_pressure0)
+            kz = prm.eddy_coef;
+          else if (pr > prm.eddy_pressure1)
+            kz = prm.eddy_coef * (pr - prm.eddy_pressure1) / (prm.eddy_pressure0 - prm.eddy_pressure1);
+          b.eddy[gidx(0, g, cl)] = kz;
+        }
         if (store) {
           b.rho[gidx(0, g, cl)] = rho;
           b.velocity[gidx(0, g, cl)] = c.x(F_VE, i);

@@ -88,13 +88,25 @@ typedef struct GitmVertParams {
                                           calc_rates.Earth.f90:34-50,
                                           calc_timestep.f90:109-118); 0 = use the
                                          arrays the caller passes            */
-  int32_t reserved0;
+  int32_t compute_eddy;               /* 1 = after each step, KappaEddyDiffusion
+                                         (GitmColumnBatch.eddy, cells 1..nAlts)
+                                         is recomputed from Pressure =
+                                         Temperature * Rho of the state the step
+                                         started from, as calc_sources does
+                                         (calc_sources.f90:26, Earth.f90:376-411,
+                                         calc_pressure.f90:23): the next step
+                                         uses it.  GITM-array form only; the
+                                         adjoint takes the eddy coefficient as
+                                         an input and refuses this mode.      */
   double beta_limiter;                /* BetaLimiter (2.0)  ModInputs.f90:104 */
   double max_vertical_velocity;       /* MaximumVerticalVelocity (1000) ModInputs.f90:224 */
   double min_tec;                     /* MinTEC (2.0)        ModInputs.f90:261 */
   double omega_body;                  /* OmegaBodyInput (2 pi / 86400 s) ModInputs.f90:285 */
   double vert_tau;                    /* VertTau (1e9 s)     ModEarth.f90:325 */
   double thermal_diff_coef[GITM_NSPECIES]; /* ThermalDiffCoefS calc_rates.Earth.f90:83-84 */
+  double eddy_coef;                   /* EddyDiffusionCoef (50 m^2/s)  ModInputs.f90:302 */
+  double eddy_pressure0;              /* EddyDiffusionPressure0 (0.01 Pa)  ModInputs.f90:303 */
+  double eddy_pressure1;              /* EddyDiffusionPressure1 (0.005 Pa) ModInputs.f90:304 */
 } GitmVertParams;
 
 /*
@@ -113,9 +125,10 @@ typedef struct GitmVertParams {
  * in which case they may be NULL):
  *   gamma (Gamma), mean_major_mass (MeanMajorMass), temp_unit (TempUnit),
  *   cmax (cMax_GDB(:,:,:,iUp_); cells 0..nAlts+1 are used)
- * Read-only inputs:
+ * Inputs (read-only unless noted):
  *   ivel_up         IVelocity(:,:,:,iUp_)
- *   eddy            KappaEddyDiffusion (cells 1..nAlts are used)
+ *   eddy            KappaEddyDiffusion (cells 1..nAlts are used; written
+ *                   when compute_eddy = 1)
  *   cos_lat, sza, mlat  [n_cols]  CosLatitude, SZA (rad), MLatitude(nAlts) (deg)
  *   lbc  [2][10][n_cols] or NULL: lower boundary values for cells -1 and 0
  *        (the MSIS call of set_vertical_bcs.Earth.f90:112-137)
@@ -146,7 +159,7 @@ typedef struct GitmColumnBatch {
   double* temp_unit;
   double* cmax;
   const double* ivel_up;
-  const double* eddy;
+  double* eddy;
   const double* cos_lat;
   const double* sza;
   const double* mlat;

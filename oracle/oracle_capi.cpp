@@ -5,8 +5,9 @@
 // it.  The per-column work follows advance_vertical (advance_vertical.f90:
 // 45-219) around advance_vertical_1d_rusanov, with the coefficient producers
 // of the GITM main loop (main.f90:56-73) in front when
-// params.compute_coefficients is set.  Columns are independent, so they are
-// split over host threads.
+// params.compute_coefficients is set, and calc_sources' eddy coefficient
+// behind it when params.compute_eddy is set.  Columns are independent, so
+// they are split over host threads.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -25,6 +26,16 @@ inline int64_t nat(int f, int g, int64_t c, int G, int64_t n) { return (int64_t(
 
 inline double grid_at(const double* p, int g, int64_t c, const GitmColumnBatch& m) {
   return m.grid_per_column ? p[int64_t(g) * m.n_cols + c] : p[g];
+}
+
+// calc_eddy_diffusion_coefficient (Earth.f90:376-411) at one cell:
+// EddyDiffusionCoef above EddyDiffusionPressure0, a linear taper down to
+// EddyDiffusionPressure1, 0 below.
+double eddy_coefficient(double pressure, const GitmVertParams& prm) {
+  if (pressure > prm.eddy_pressure0) return prm.eddy_coef;
+  if (pressure > prm.eddy_pressure1)
+    return prm.eddy_coef * (pressure - prm.eddy_pressure1) / (prm.eddy_pressure0 - prm.eddy_pressure1);
+  return 0.0;
 }
 
 template <class R>
@@ -74,6 +85,10 @@ uint32_t step_gitm_column(const GitmVertParams& prm, const GitmColumnBatch& m, i
         ww[s * G + g] = m.vert_vel[nat(s, g, c, G, n)];
       }
     for (int g = 0; g < G; ++g) tt[g] = m.temperature[nat(0, g, c, G, n)];
+    // Pressure = Temperature * Rho (calc_pressure.f90:23) of the state the
+    // step starts from, for calc_sources' eddy coefficient after the step
+    std::vector<double> pressure(G);
+    for (int g = 0; g < G; ++g) pressure[g] = tt[g] * m.rho[nat(0, g, c, G, n)];
     if (prm.compute_coefficients) {
       Producers pr;
       produce_coefficients(nAlts, nden.data(), tt.data(), ww.data(), pr);
@@ -163,6 +178,10 @@ uint32_t step_gitm_column(const GitmVertParams& prm, const GitmColumnBatch& m, i
       }
     }
     if (!finite) status |= GITM_ST_NONFINITE;
+    // calc_sources.f90:26 after the vertical advance: the next step's
+    // KappaEddyDiffusion (cells 1..nAlts, the ones the solver reads)
+    if (prm.compute_eddy)
+      for (int g = 2; g <= nAlts + 1; ++g) m.eddy[nat(0, g, c, G, n)] = eddy_coefficient(pressure[g], prm);
   }
   return status;
 }

@@ -78,6 +78,50 @@ def test_heating_update(torch_cuda, oracle_lib, n_steps):
     assert_state_close(out, ref, STATE, rtol=1e-10 if n_steps == 1 else 1e-9)
 
 
+@pytest.mark.parametrize("solver", [abi.SOLVER_RUSANOV, abi.SOLVER_AUSM])
+@pytest.mark.parametrize("n_steps,spl", [(1, 1), (4, 4), (4, 1)])
+def test_eddy_producer(torch_cuda, oracle_lib, solver, n_steps, spl):
+    """compute_eddy: KappaEddyDiffusion(1:nAlts) recomputed after every step
+    from the pressure the step started from (calc_sources), read by the next
+    step, resident steps included; with the heating line on."""
+    p = abi.default_params(compute_eddy=1, solver=solver)
+    m = synthetic.make_member(64, 50, seed=35, with_heating=True)
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0, n_steps=n_steps)
+    out, st = gpu_advance(m, p, 2.0, n_steps=n_steps, config=dict(steps_per_launch=spl))
+    assert_state_close(out, ref, STATE + ("eddy",), rtol=1e-10 if n_steps == 1 else 1e-9)
+    np.testing.assert_array_equal(st, st_ref)
+    # the produced profile is not the one passed in
+    assert np.abs(out["eddy"] - m.eddy).max() > 0.0
+
+
+def test_eddy_producer_host_path(torch_cuda):
+    """The host-pointer form copies the produced coefficient back."""
+    from gitm_b200 import vertical as V
+    p = abi.default_params(compute_eddy=1)
+    m = synthetic.make_member(700, 50, seed=36)
+    # the launch shape of the host-pointer form: 128 threads, one step per launch
+    dev_out, _ = gpu_advance(m, p, 2.0, n_steps=2, config=dict(threads=128, steps_per_launch=1))
+    h = m.copy()
+    ctx = V.VerticalContext(p)
+    V.advance_vertical_all_host(ctx, [h], 2.0, n_steps=2)
+    for k in synthetic.Member.STATE + ("eddy",):
+        np.testing.assert_array_equal(getattr(h, k), dev_out[k], err_msg=k)
+    ctx.close()
+
+
+def test_eddy_producer_refused_by_adjoint(torch_cuda):
+    """The adjoint differentiates a step with the eddy coefficient as an input."""
+    from gitm_b200 import adjoint as AD
+    from gitm_b200 import vertical as V
+    ctx = V.VerticalContext(abi.default_params(compute_eddy=1))
+    run = AD.StepRunner(ctx, synthetic.make_member(8, 50, seed=37), 2.0, autotune=False)
+    st = run.state()
+    with pytest.raises(V.GitmError):
+        run.vjp(st, {})
+    run.close()
+    ctx.close()
+
+
 def test_msis_lower_boundary(torch_cuda, oracle_lib):
     p = abi.default_params(use_msis_bcs=1)
     m = synthetic.make_member(64, 50, seed=22, with_lbc=True)

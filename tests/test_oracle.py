@@ -139,3 +139,44 @@ def test_oracle_heating_update(oracle_lib):
     np.testing.assert_allclose(d[0, 2:-2], want[0, 2:-2], rtol=1e-9,
                                atol=4e-16 * np.abs(b.temperature).max())
     assert np.abs(d[0, [0, 1, -2, -1]]).max() == 0.0
+
+
+def _eddy_profile(pressure, p):
+    """calc_eddy_diffusion_coefficient (Earth.f90:376-411), numpy form."""
+    k = np.zeros_like(pressure)
+    taper = p.eddy_coef * (pressure - p.eddy_pressure1) / (p.eddy_pressure0 - p.eddy_pressure1)
+    k = np.where(pressure > p.eddy_pressure1, taper, k)
+    return np.where(pressure > p.eddy_pressure0, p.eddy_coef, k)
+
+
+def test_oracle_eddy_producer(oracle_lib):
+    """compute_eddy: after a step, KappaEddyDiffusion(1:nAlts) is the profile
+    of Pressure = Temperature * Rho at the start of that step; the step itself
+    reads the coefficient passed in, the next step the produced one."""
+    from gitm_b200 import abi, synthetic
+    m = synthetic.make_member(16, 50, seed=8, with_heating=True)
+    p = abi.default_params(compute_eddy=1)
+    p0 = abi.default_params()
+    pressure = m.temperature * m.rho
+    want = _eddy_profile(pressure, p)
+    # the synthetic columns cover all three regimes of the profile
+    inner = pressure[0, 2:-2]
+    assert (inner > p.eddy_pressure0).any() and (inner <= p.eddy_pressure1).any()
+    assert ((inner > p.eddy_pressure1) & (inner <= p.eddy_pressure0)).any()
+    a, b = m.copy(), m.copy()
+    oracle_lib.advance(a, p, 2.0, 1)
+    oracle_lib.advance(b, p0, 2.0, 1)
+    for k in synthetic.Member.STATE:
+        np.testing.assert_array_equal(getattr(a, k), getattr(b, k), err_msg=k)
+    np.testing.assert_array_equal(a.eddy[0, 2:-2], want[0, 2:-2])
+    np.testing.assert_array_equal(a.eddy[0, [0, 1, -2, -1]], m.eddy[0, [0, 1, -2, -1]])
+    # two steps = one step, the produced coefficient, one more step
+    two = m.copy()
+    oracle_lib.advance(two, p, 2.0, 2)
+    c = b.copy()
+    c.eddy[0, 2:-2] = want[0, 2:-2]
+    p1 = c.temperature * c.rho
+    oracle_lib.advance(c, p0, 2.0, 1)
+    for k in synthetic.Member.STATE:
+        np.testing.assert_array_equal(getattr(two, k), getattr(c, k), err_msg=k)
+    np.testing.assert_array_equal(two.eddy[0, 2:-2], _eddy_profile(p1, p)[0, 2:-2])
