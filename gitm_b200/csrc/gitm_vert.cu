@@ -19,6 +19,7 @@
 #include "vert_common.cuh"
 #include "vert_kernel.cuh"
 #include "vert_adjoint.cuh"
+#include "vert_instances.h"
 
 using namespace gv;
 
@@ -232,34 +233,26 @@ static bool acc_global(int threads) {
   return false;
 }
 
-template <int IO, int SOLVER>
-static const void* kernel_for_t(int threads) {
-  if constexpr (SOLVER == GITM_SOLVER_AUSM) {
-    // the AUSM stage holds more state per cell: two shapes
-    switch (threads) {
-      case 128: return (const void*)vert_step_kernel<IO, 128, 2, true, SOLVER>;
-      case 256: return (const void*)vert_step_kernel<IO, 256, 1, false, SOLVER>;
-      default: return nullptr;
-    }
-  } else {
-    switch (threads) {
-      case 128: return (const void*)vert_step_kernel<IO, 128, 3, true, SOLVER>;
-      case 160: return (const void*)vert_step_kernel<IO, 160, 2, true, SOLVER>;
-      case 192: return (const void*)vert_step_kernel<IO, 192, 2, true, SOLVER>;
-      case 256: return (const void*)vert_step_kernel<IO, 256, 1, false, SOLVER>;
-      case 320: return (const void*)vert_step_kernel<IO, 320, 1, false, SOLVER>;
-      case 384: return (const void*)vert_step_kernel<IO, 384, 1, false, SOLVER>;
-      default: return nullptr;
-    }
-  }
-}
+// The step kernels, each compiled in its own translation unit
+// (vert_instance.cu, one per GV_STEP_INSTANCES entry).
+struct StepInstance {
+  int io, threads, solver;
+  bool save;
+  const void* (*fn)();
+  cudaError_t (*consts)(const Consts&);
+};
+static const StepInstance kInstances[] = {
+#define GV_TABLE_ENTRY(id, IO, NT, MINB, ACC, SOLVER, SAVE) {IO, NT, SOLVER, SAVE, step_kernel_##id, step_consts_##id},
+    GV_STEP_INSTANCES(GV_TABLE_ENTRY)
+#undef GV_TABLE_ENTRY
+};
 
 // The step kernel for an array form (0 GITM arrays, 1 ModVertical), solver
 // and CTA size, or nullptr when that shape is not built.
 static const void* kernel_for(int io, int solver, int threads) {
-  if (solver == GITM_SOLVER_AUSM)
-    return io ? kernel_for_t<1, GITM_SOLVER_AUSM>(threads) : kernel_for_t<0, GITM_SOLVER_AUSM>(threads);
-  return io ? kernel_for_t<1, GITM_SOLVER_RUSANOV>(threads) : kernel_for_t<0, GITM_SOLVER_RUSANOV>(threads);
+  for (const StepInstance& k : kInstances)
+    if (!k.save && k.io == io && k.solver == solver && k.threads == threads) return k.fn();
+  return nullptr;
 }
 
 // ------------------------------------------------------------------ API
@@ -329,6 +322,8 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
   fill_consts(k);
   if (cudaMemcpyToSymbol(c_k, &k, sizeof k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
   if (adjoint_set_consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
+  for (const StepInstance& si : kInstances)
+    if (si.consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
   for (int t : kThreadChoices)
     for (int io = 0; io < 2; ++io)
       for (int solver : {GITM_SOLVER_RUSANOV, GITM_SOLVER_AUSM})
@@ -1668,7 +1663,7 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   kp.prm = ctx->params;
   void* args[] = {&kp};
   const int grid = std::min(n_tiles, kNoAllocSlots);
-  CUDA_TRY(ctx, cudaLaunchKernel((const void*)vert_step_kernel<0, kNoAllocThreads, 3, true, GITM_SOLVER_RUSANOV>, dim3(grid),
+  CUDA_TRY(ctx, cudaLaunchKernel(kernel_for(0, GITM_SOLVER_RUSANOV, kNoAllocThreads), dim3(grid),
                                  dim3(kNoAllocThreads), args, smem, st));
   return GITM_OK;
 }

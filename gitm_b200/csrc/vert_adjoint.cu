@@ -4,22 +4,24 @@
 // (rusanov_cell, bc_column, friction_solve, ...).  Compiled in the same
 // translation unit, its instantiation changes how those functions are
 // compiled into the forward kernel (a 400-byte local-memory frame and a
-// slower step), so it is built here, apart.  Without relocatable device
-// code this unit has its own copy of the constant table c_k, which the host
-// sets through adjoint_set_consts when a context is created.
+// slower step), so it is built here, apart, as every step kernel is.
+// Without relocatable device code this unit has its own copy of the
+// constant table c_k, which the host sets through adjoint_set_consts when a
+// context is created.
 #include "vert_common.cuh"
 #include "vert_kernel.cuh"
 #include "vert_adjoint.cuh"
+#include "vert_instances.h"
 
 namespace gv {
 
 const void* adjoint_kernel_fn() { return (const void*)vert_adjoint_kernel<ADJ_THREADS>; }
 
 // The step kernel that also saves the stage states for the adjoint (GITM
-// arrays, Rusanov, 128 threads, accumulator in per-CTA scratch).
-const void* saving_kernel_fn() {
-  return (const void*)vert_step_kernel<0, ADJ_THREADS, 3, true, GITM_SOLVER_RUSANOV, true>;
-}
+// arrays, Rusanov, 128 threads, accumulator in per-CTA scratch), built in a
+// translation unit of its own like the other step kernels.
+static_assert(ADJ_THREADS == 128, "the saving step kernel is built for 128 threads");
+const void* saving_kernel_fn() { return step_kernel_rus0_t128_save(); }
 
 cudaError_t adjoint_set_consts(const Consts& k) { return cudaMemcpyToSymbol(c_k, &k, sizeof k); }
 

@@ -683,10 +683,10 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
       if constexpr (SAVE) {
         const int per = NF * G + NPAS * NPC;
         const int xo = cur ? L.X1 : L.X0;
-        for (int w = tid; w < nc * per; w += NT) {
-          const int cl = w / per, r = w - cl * per;
-          const int64_t gcol = M.col_offset + tile.c0 + cl;
-          kp.save[(int64_t(s) * kp.save_ncols + gcol) * kp.save_per + r] = sm[size_t(L.stride) * cl + xo + r];
+        for (int cl = 0; cl < nc; ++cl) {
+          const double* src = sm + size_t(L.stride) * cl + xo;
+          double* dst = kp.save + (int64_t(s) * kp.save_ncols + M.col_offset + tile.c0 + cl) * kp.save_per;
+          for (int r = tid; r < per; r += NT) dst[r] = src[r];
         }
       }
     };

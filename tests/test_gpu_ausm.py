@@ -111,7 +111,8 @@ def test_ausm_host_pointer_path(torch_cuda):
     from gitm_b200 import vertical as V
     p = ausm()
     m = synthetic.make_member(700, 50, seed=49)
-    dev_out, _ = gpu_advance(m, p, 2.0)
+    # the launch shape of the host-pointer form (each shape is compiled on its own)
+    dev_out, _ = gpu_advance(m, p, 2.0, config=dict(threads=128, steps_per_launch=1))
     h = m.copy()
     ctx = V.VerticalContext(p)
     V.advance_vertical_all_host(ctx, [h], 2.0)

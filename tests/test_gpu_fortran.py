@@ -115,11 +115,18 @@ def test_fortran_layout_matches_native(on_device):
             m.cos_lat[row] = m.cos_lat[b * 81 + j * 9]
     f = fortran_arrays(m)
     ns_in = f["ndensity_s"].copy()
-    # native reference on the same columns
+    # native reference on the same columns, through the entry point the
+    # Fortran form calls (device arrays: gitm_vert_advance_native; host
+    # arrays: gitm_vert_advance_native_host), so that the same kernel runs
     ctx = V.VerticalContext(p)
-    dm = V.device_member(m)
-    V.advance_vertical_all(ctx, [dm], 2.0)
-    ref = dm.to_numpy()
+    if on_device:
+        dm = V.device_member(m)
+        V.advance_vertical_all(ctx, [dm], 2.0)
+        ref = dm.to_numpy()
+    else:
+        h = m.copy()
+        V.advance_vertical_all_host(ctx, [h], 2.0)
+        ref = dict(h.arrays())
     for blk in range(1, NBLK + 1):
         # MeanMajorMass / TempUnit hold one block (calc_rates(iBlock)): give
         # the descriptor this block's slice through a zero block stride
