@@ -445,37 +445,49 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
 }
 
 // ---------------------------------------------------------------- stage^T
-// Reverse of rusanov_cell at interior cell i: kb[f] is the adjoint of the
-// increment New - state of field f; contributions go to the state adjoint
-// (this cell and its neighbours), the slope adjoints, the cMax and Gamma
-// adjoints; returns the KappaEddyDiffusion adjoint of the cell.
-__device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, int i, const GitmVertParams& prm,
-                                              double dt, double eddy, double ivup, const double (&kb)[NF]) {
-  const int G = c.L.G;
-  const int nA = c.L.nAlts;
-  const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
-  const double idc = c.g(GC_IDC, i);
-  const double cmm = c.cm(i - 1), cm0 = c.cm(i), cmp = c.cm(i + 1);
-  const double fc0 = 0.5 * fmax(cmm, cm0);
-  const double fc1 = 0.5 * fmax(cm0, cmp);
-  auto sweep = [&](int f, double& grad, double& diff) {
-    const double* v = &c.col[c.xo + f * G + 1];
-    const double* d = &c.col[c.L.DL + f * (nA + 2)];
+// Reverse of rusanov_cell at interior cell i, in two passes that each hold
+// only their own part of the cell's values (one pass over everything held
+// the friction matrix, the species terms and all field adjoints at once and
+// spilled): cell_adjoint_species (continuity and momentum of the species,
+// the friction solve, LogRho) and cell_adjoint_rest (temperature, the
+// horizontal winds, the bulk vertical wind's own terms, the ions).  kb(f)
+// is the adjoint of New for field f (the caller applies K = New - state);
+// contributions go to the state adjoint (this cell and its neighbours), the
+// slope adjoints, the cMax and Gamma adjoints.  Every sweep adjoint is
+// linear in its inputs, so the two passes' shares of the temperature
+// sweep add up.
+
+// The face geometry of cell i and its sweep (calc_rusanov_alts_rusanov,
+// vertical_solver_rusanov.f90:694-718), forward and reverse.
+struct CellFaces {
+  double dF0, dF1, idc, fc0, fc1;
+  double fc0b, fc1b;  // adjoints of the two dissipation coefficients
+
+  __device__ __forceinline__ CellFaces(const ColCtx& c, int i) {
+    dF0 = c.dAF(i);
+    dF1 = c.dAF(i + 1);
+    idc = c.g(GC_IDC, i);
+    fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
+    fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
+    fc0b = 0.0;
+    fc1b = 0.0;
+  }
+  __device__ __forceinline__ void sweep(const ColCtx& c, int f, int i, double& grad, double& diff) const {
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
     const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
     const double R0 = v[i] - 0.5 * d[i] * dF0;
     const double L1 = v[i] + 0.5 * d[i] * dF1;
     const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
     grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
     diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
-  };
-  double fc0b = 0.0, fc1b = 0.0;
-  double self[NF];
-#pragma unroll
-  for (int f = 0; f < NF; ++f) self[f] = 0.0;
-  // adjoint of one sweep: (gb, db) -> faces -> values and slopes
-  auto sweep_adj = [&](int f, double gb, double dbv) {
-    const double* v = &c.col[c.xo + f * G + 1];
-    const double* d = &c.col[c.L.DL + f * (nA + 2)];
+  }
+  // (gb, dbv) -> faces -> values and slopes; returns this cell's own share
+  // of the value adjoint (the neighbours' shares go in by atomics)
+  __device__ __forceinline__ double sweep_adj(const ColCtx& c, const ColAdj& a, int f, int i, double gb,
+                                              double dbv) {
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
     const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
     const double R0 = v[i] - 0.5 * d[i] * dF0;
     const double L1 = v[i] + 0.5 * d[i] * dF1;
@@ -487,39 +499,50 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
     fc0b += -idc * (R0 - L0) * dbv;
     a.add(f, i - 1, L0b);
     a.dadd(f, i - 1, 0.5 * dF0 * L0b);
-    self[f] += R0b + L1b;
     a.dadd(f, i, -0.5 * dF0 * R0b + 0.5 * dF1 * L1b);
     a.add(f, i + 1, R1b);
     a.dadd(f, i + 1, -0.5 * dF1 * R1b);
-  };
+    return R0b + L1b;
+  }
+  // cMax through the dissipation coefficients (the branch of each max the
+  // forward took)
+  __device__ __forceinline__ void cmax_adj(const ColCtx& c, const ColAdj& a, int i) const {
+    const double cmm = c.cm(i - 1), cm0 = c.cm(i), cmp = c.cm(i + 1);
+    if (cmm >= cm0) atomicAdd(&a.cmb[i], 0.5 * fc0b); else atomicAdd(&a.cmb[i + 1], 0.5 * fc0b);
+    if (cm0 >= cmp) atomicAdd(&a.cmb[i + 1], 0.5 * fc1b); else atomicAdd(&a.cmb[i + 2], 0.5 * fc1b);
+  }
+};
 
+// Species continuity and momentum (:548-617), the friction solve
+// (calc_neutral_friction.f90:47-106), the clamp and LogRho / the bulk wind's
+// species terms (:643-658) in reverse.  kb(f) = kbp[f * kstride].  Returns
+// the KappaEddyDiffusion adjoint of the cell.
+__device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, int i, const GitmVertParams& prm,
+                                              double dt, double eddy, const double* kbp, int kstride) {
+  auto kb = [&](int f) { return kbp[size_t(f) * kstride]; };
+  CellFaces fa(c, i);
   // ---- forward recompute
   const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
-  const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i), VU = c.x(F_VU, i);
+  const double T = c.x(F_T, i), VE = c.x(F_VE, i), VN = c.x(F_VN, i);
   const double LR = c.x(F_LRHO, i);
-  const double gm = c.gm(i);
-  double gT, dT, gE, dE, gN, dN, gU, dU;
-  sweep(F_T, gT, dT);
-  sweep(F_VE, gE, dE);
-  sweep(F_VN, gN, dN);
-  sweep(F_VU, gU, dU);
-  const double divv = gU + 2 * VU * invr;
+  double gT, dT;
+  fa.sweep(c, F_T, i, gT, dT);
   const double itau = 1.0 / (prm.use_damping ? 15 - (1 - exp(-1.0 * c.g(GC_ALT, i) / 1000.0 / 40.0)) * 5.0
                                              : prm.vert_tau);
   const double hz = (VN * VN + VE * VE) * invr;
   const double cor = prm.use_coriolis ? dt * (c.sc(SC_CENT) * rr + c.sc(SC_CORI) * VE) : 0.0;
-  double wv[NS], enl[NS];
+  double wv[NS], menl[NS];
   double sumrho = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     double gL, dL, gW, dW;
-    sweep(F_LNS + s, gL, dL);
-    sweep(F_W + s, gW, dW);
+    fa.sweep(c, F_LNS + s, i, gL, dL);
+    fa.sweep(c, F_W + s, i, gW, dW);
     const double Ls = c.x(F_LNS + s, i), Ws = c.x(F_W + s, i);
     const double divw = gW + 2 * Ws * invr;
     const double nl = Ls - dt * (divw + Ws * gL) + dt * dL;
-    enl[s] = exp(nl);
-    sumrho = sumrho + c_k.mass[s] * enl[s];
+    menl[s] = c_k.mass[s] * exp(nl);
+    sumrho = sumrho + menl[s];
     const double km = c_k.k_over_m[s];
     double w = Ws - dt * (Ws * gW - hz + T * gL * km + gT * km - grav) + dt * dW - Ws * itau;
     w = w + cor;
@@ -530,10 +553,22 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
 #pragma unroll
   for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
   const double ir = exp(-LR);
-  double glc[NS], vsol[NS], lu[NS][NS], pw[NS];
-  const double lt = log(T);
+  // reverse of New LogRho = log(sumrho): the continuity adjoints
+  double nlb[NS];
+  {
+    const double srb = kb(F_LRHO) / sumrho;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) nlb[s] = srb * menl[s];
+  }
+  double Tb = 0.0, VEb = 0.0, VNb = 0.0, LRb = 0.0, irb = 0.0;
+  double nsb[NS], wb[NS], lself[NS];  // lself: GradLogConS's share of this cell's LogNS adjoint
+  double eddyb = 0.0;
+  // New VU = sum_s w_s m_s ns_s / Rho; New VertVel = the clamped w
+  const double kvu = kb(F_VU);
   if (prm.use_neutral_friction) {
+    double glc[NS], lu[NS][NS], vsol[NS], pw[NS];
     grad_log_cons(c, i, glc);
+    const double lt = log(T);
 #pragma unroll
     for (int e = 0; e < NS; ++e) pw[e] = exp(c_k.one_minus_e[e] * lt);
 #pragma unroll
@@ -548,16 +583,20 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
       }
       lu[r][r] = 1.0 + dt * rs;
     }
-    // LU without pivoting, multipliers kept below the diagonal
+    // LU without pivoting: multipliers below the diagonal, pivot
+    // reciprocals on it (as friction_solve)
 #pragma unroll
-    for (int p = 0; p < NS; ++p)
+    for (int p = 0; p < NS; ++p) {
+      const double ip = 1.0 / lu[p][p];
+      lu[p][p] = ip;
 #pragma unroll
       for (int r = p + 1; r < NS; ++r) {
-        const double l = lu[r][p] / lu[p][p];
+        const double l = lu[r][p] * ip;
         lu[r][p] = l;
 #pragma unroll
         for (int q = p + 1; q < NS; ++q) lu[r][q] -= l * lu[p][q];
       }
+    }
 #pragma unroll
     for (int r = 0; r < NS; ++r) {
       double sum = wv[r];
@@ -570,55 +609,35 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
       double sum = vsol[r];
 #pragma unroll
       for (int q = r + 1; q < NS; ++q) sum -= lu[r][q] * vsol[q];
-      vsol[r] = sum / lu[r][r];
+      vsol[r] = sum * lu[r][r];
     }
-  } else {
+    // clamp, bulk wind and their reverse
+    double vb[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      vsol[s] = wv[s];
-      glc[s] = 0.0;
-    }
-  }
-  double wc[NS];
-  bool inside[NS];
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const double v = prm.use_neutral_friction ? vsol[s] + (-eddy * glc[s]) : vsol[s];
-    inside[s] = !(v < -prm.max_vertical_velocity) && !(v > prm.max_vertical_velocity);
-    double w = fmax(-prm.max_vertical_velocity, v);
-    wc[s] = fmin(prm.max_vertical_velocity, w);
-  }
-
-  // ---- reverse
-  double Tb = 0.0, VEb = 0.0, VNb = 0.0, VUb = 0.0, LRb = 0.0, irb = 0.0;
-  double Lb[NS], Wb[NS], nsb[NS], nlb[NS], wcb[NS];
-  // kb is the adjoint of the new values (the caller applies K = New - state)
-  // New LogRho = log(sumrho)
-  const double srb = kb[F_LRHO] / sumrho;
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    nlb[s] = srb * c_k.mass[s] * enl[s];
-    Lb[s] = 0.0;
-    Wb[s] = 0.0;
-    nsb[s] = 0.0;
-  }
-  // New VU = sum_s w_s m_s ns_s / Rho; New VertVel = the clamped w
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const double m = c_k.mass[s];
-    wcb[s] = kb[F_VU] * (m * ns[s] * ir) + kb[F_W + s];
-    nsb[s] += kb[F_VU] * wc[s] * m * ir;
-    irb += kb[F_VU] * wc[s] * m * ns[s];
-  }
-  double wb[NS];
-  double eddyb = 0.0;
-  if (prm.use_neutral_friction) {
-    double vb[NS], glcb[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      vb[s] = inside[s] ? wcb[s] : 0.0;
+      const double v = vsol[s] + (-eddy * glc[s]);
+      const bool inside = !(v < -prm.max_vertical_velocity) && !(v > prm.max_vertical_velocity);
+      double wc = fmax(-prm.max_vertical_velocity, v);
+      wc = fmin(prm.max_vertical_velocity, wc);
+      const double m = c_k.mass[s];
+      const double wcb = kvu * (m * ns[s] * ir) + kb(F_W + s);
+      nsb[s] = kvu * wc * m * ir;
+      irb += kvu * wc * m * ns[s];
+      vb[s] = inside ? wcb : 0.0;
       eddyb -= vb[s] * glc[s];
-      glcb[s] = -eddy * vb[s];
+    }
+    // GradLogConS: 5-point mesh on log(m_s) + LogNS - LogRho
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const double mc = c.g(GC_M0 + q, i);
+      double lrb = 0.0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double v = (-eddy * vb[s]) * mc;
+        lrb -= v;
+        if (q == 2) lself[s] = v; else a.add(F_LNS + s, i - 2 + q, v);
+      }
+      if (q == 2) LRb += lrb; else a.add(F_LRHO, i - 2 + q, lrb);
     }
     // wb = M^-T vb with M = L U: U^T z = vb, then L^T wb = z
 #pragma unroll
@@ -626,7 +645,7 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
       double sum = vb[r];
 #pragma unroll
       for (int q = 0; q < r; ++q) sum -= lu[q][r] * wb[q];
-      wb[r] = sum / lu[r][r];
+      wb[r] = sum * lu[r][r];
     }
 #pragma unroll
     for (int r = NS - 1; r >= 0; --r) {
@@ -653,34 +672,32 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
 #pragma unroll
     for (int e = 0; e < NS; ++e) ltb += pwb[e] * pw[e] * c_k.one_minus_e[e];
     Tb += ltb / T;
-    // GradLogConS: 5-point mesh on log(m_s) + LogNS - LogRho
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      const double mc = c.g(GC_M0 + q, i);
-      double lrb = 0.0;
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const double v = glcb[s] * mc;
-        lrb -= v;
-        if (q == 2) Lb[s] += v; else a.add(F_LNS + s, i - 2 + q, v);
-      }
-      if (q == 2) LRb += lrb; else a.add(F_LRHO, i - 2 + q, lrb);
-    }
   } else {
 #pragma unroll
-    for (int s = 0; s < NS; ++s) wb[s] = inside[s] ? wcb[s] : 0.0;
+    for (int s = 0; s < NS; ++s) {
+      const double v = wv[s];
+      const bool inside = !(v < -prm.max_vertical_velocity) && !(v > prm.max_vertical_velocity);
+      double wc = fmax(-prm.max_vertical_velocity, v);
+      wc = fmin(prm.max_vertical_velocity, wc);
+      const double m = c_k.mass[s];
+      const double wcb = kvu * (m * ns[s] * ir) + kb(F_W + s);
+      nsb[s] = kvu * wc * m * ir;
+      irb += kvu * wc * m * ns[s];
+      wb[s] = inside ? wcb : 0.0;
+      lself[s] = 0.0;
+    }
   }
   // species momentum, continuity and their sweeps
   double gTb = 0.0, hzb = 0.0, corb = 0.0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     double gL, dL, gW, dW;
-    sweep(F_LNS + s, gL, dL);
-    sweep(F_W + s, gW, dW);
+    fa.sweep(c, F_LNS + s, i, gL, dL);
+    fa.sweep(c, F_W + s, i, gW, dW);
     const double Ws = c.x(F_W + s, i);
     const double km = c_k.k_over_m[s];
     const double w = wb[s];
-    Wb[s] += w * (1.0 - dt * gW - itau);
+    double Wb = w * (1.0 - dt * gW - itau);
     double gWb = -dt * Ws * w;
     hzb += dt * w;
     Tb += -dt * gL * km * w;
@@ -689,61 +706,76 @@ __device__ inline double rusanov_cell_adjoint(const ColCtx& c, const ColAdj& a, 
     const double dWb = dt * w;
     corb += w;
     // New LogNS = nl = Ls - dt (divw + Ws gL) + dt dL
-    const double n = nlb[s] + kb[F_LNS + s];
-    Lb[s] += n;
+    const double n = nlb[s] + kb(F_LNS + s);
+    double Lb = lself[s] + n;
     const double divwb = -dt * n;
-    Wb[s] += -dt * gL * n + 2 * invr * divwb;
+    Wb += -dt * gL * n + 2 * invr * divwb;
     gLb += -dt * Ws * n;
     const double dLb = dt * n;
     gWb += divwb;
-    sweep_adj(F_LNS + s, gLb, dLb);
-    sweep_adj(F_W + s, gWb, dWb);
-    Lb[s] += nsb[s] * ns[s];
+    Lb += fa.sweep_adj(c, a, F_LNS + s, i, gLb, dLb);
+    Wb += fa.sweep_adj(c, a, F_W + s, i, gWb, dWb);
+    Lb += nsb[s] * ns[s];
+    a.add(F_LNS + s, i, Lb);
+    a.add(F_W + s, i, Wb);
   }
   LRb -= irb * ir;
   if (prm.use_coriolis) VEb += corb * dt * c.sc(SC_CORI);
   VNb += hzb * 2 * VN * invr;
   VEb += hzb * 2 * VE * invr;
+  // the species' share of the temperature sweep
+  Tb += fa.sweep_adj(c, a, F_T, i, gTb, 0.0);
+  fa.cmax_adj(c, a, i);
+  a.add(F_T, i, Tb);
+  a.add(F_VE, i, VEb);
+  a.add(F_VN, i, VNb);
+  a.add(F_LRHO, i, LRb);
+  return eddyb;
+}
+
+// Temperature, horizontal winds, the bulk vertical wind's own terms and the
+// ions (:557-568, :660-680) in reverse.
+__device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i, double dt, double ivup,
+                                         const double* kbp, int kstride) {
+  auto kb = [&](int f) { return kbp[size_t(f) * kstride]; };
+  CellFaces fa(c, i);
+  const double invr = c.g(GC_INVR, i);
+  const double T = c.x(F_T, i), VU = c.x(F_VU, i);
+  const double gm = c.gm(i);
+  double gT, dT, gE, dE, gN, dN, gU, dU;
+  fa.sweep(c, F_T, i, gT, dT);
+  fa.sweep(c, F_VE, i, gE, dE);
+  fa.sweep(c, F_VN, i, gN, dN);
+  fa.sweep(c, F_VU, i, gU, dU);
+  const double divv = gU + 2 * VU * invr;
   // ions: New = I - dt (IVel gI) + dt dI
 #pragma unroll
   for (int s = 0; s < NADV; ++s) {
-    self[F_I + s] += kb[F_I + s];
-    sweep_adj(F_I + s, -dt * ivup * kb[F_I + s], dt * kb[F_I + s]);
+    const double k = kb(F_I + s);
+    const double own = fa.sweep_adj(c, a, F_I + s, i, -dt * ivup * k, dt * k);
+    a.add(F_I + s, i, k + own);
   }
   // horizontal winds: New = V - dt VU gV + dt dV
-  VEb += kb[F_VE];
-  VNb += kb[F_VN];
-  VUb += -dt * gE * kb[F_VE] - dt * gN * kb[F_VN];
-  sweep_adj(F_VE, -dt * VU * kb[F_VE], dt * kb[F_VE]);
-  sweep_adj(F_VN, -dt * VU * kb[F_VN], dt * kb[F_VN]);
+  const double kE = kb(F_VE), kN = kb(F_VN), kT = kb(F_T);
+  double VEb = kE + fa.sweep_adj(c, a, F_VE, i, -dt * VU * kE, dt * kE);
+  double VNb = kN + fa.sweep_adj(c, a, F_VN, i, -dt * VU * kN, dt * kN);
+  double VUb = -dt * gE * kE - dt * gN * kN;
   // temperature: New = T - dt (VU gT + (Gamma - 1) T divv) + dt dT
-  Tb += kb[F_T];
-  VUb += -dt * gT * kb[F_T];
-  gTb += -dt * VU * kb[F_T];
-  const double gmb = -dt * T * divv * kb[F_T];
-  Tb += -dt * (gm - 1.0) * divv * kb[F_T];
-  const double divvb = -dt * (gm - 1.0) * T * kb[F_T];
+  double Tb = kT;
+  VUb += -dt * gT * kT;
+  const double gTb = -dt * VU * kT;
+  const double gmb = -dt * T * divv * kT;
+  Tb += -dt * (gm - 1.0) * divv * kT;
+  const double divvb = -dt * (gm - 1.0) * T * kT;
   VUb += 2 * invr * divvb;
-  sweep_adj(F_T, gTb, dt * kb[F_T]);
-  sweep_adj(F_VU, divvb, 0.0);
-  // cMax through the dissipation coefficients
-  if (cmm >= cm0) atomicAdd(&a.cmb[i], 0.5 * fc0b); else atomicAdd(&a.cmb[i + 1], 0.5 * fc0b);
-  if (cm0 >= cmp) atomicAdd(&a.cmb[i + 1], 0.5 * fc1b); else atomicAdd(&a.cmb[i + 2], 0.5 * fc1b);
+  Tb += fa.sweep_adj(c, a, F_T, i, gTb, dt * kT);
+  VUb += fa.sweep_adj(c, a, F_VU, i, divvb, 0.0);
+  fa.cmax_adj(c, a, i);
   a.gmb[i + 1] += gmb;
-  // this cell's own contributions
-  self[F_T] += Tb;
-  self[F_VE] += VEb;
-  self[F_VN] += VNb;
-  self[F_VU] += VUb;
-  self[F_LRHO] += LRb;
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    self[F_LNS + s] += Lb[s];
-    self[F_W + s] += Wb[s];
-  }
-#pragma unroll
-  for (int f = 0; f < NF; ++f) a.add(f, i, self[f]);
-  return eddyb;
+  a.add(F_T, i, Tb);
+  a.add(F_VE, i, VEb);
+  a.add(F_VN, i, VNb);
+  a.add(F_VU, i, VUb);
 }
 
 // Adjoint of the limited slopes of cell i (interior: 4th-order form; cells 0
@@ -781,6 +813,15 @@ __device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, d
     }
   }
 }
+
+// 8-byte asynchronous global -> shared copy (cp.async: no register round
+// trip, every copy of a thread in flight at once); cp_async_wait_all waits
+// for the calling thread's copies.
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- the kernel
 template <int NT>
@@ -851,15 +892,29 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       return cta + (size_t(s) * kp.nc_max + cl) * kp.per_max;
     };
     auto save = [&](int s, int off) {
-      for (int w = tid; w < nc * per; w += NT) {
-        const int cl = w / per, r = w - cl * per;
-        state(s, cl)[r] = sm[size_t(A.stride) * cl + off + r];
+      for (int cl = 0; cl < nc; ++cl) {
+        const double* src = sm + size_t(A.stride) * cl + off;
+        double* dst = state(s, cl);
+        for (int r = tid; r < per; r += NT) dst[r] = src[r];
       }
     };
+    // (the caller's barrier publishes the copies)
     auto load = [&](int s, int off) {
-      for (int w = tid; w < nc * per; w += NT) {
-        const int cl = w / per, r = w - cl * per;
-        sm[size_t(A.stride) * cl + off + r] = state(s, cl)[r];
+      for (int cl = 0; cl < nc; ++cl) {
+        const double* src = state(s, cl);
+        double* dst = sm + size_t(A.stride) * cl + off;
+        for (int r = tid; r < per; r += NT) cp_async8(dst + r, src + r);
+      }
+      cp_async_wait_all();
+    };
+    // dst[r] += src[r], src[r] = 0 over the state-sized slots of every column
+    auto fold = [&](int dst_off, int src_off) {
+      for (int cl = 0; cl < nc; ++cl) {
+        double* col = sm + size_t(A.stride) * cl;
+        for (int r = tid; r < per; r += NT) {
+          col[dst_off + r] += col[src_off + r];
+          col[src_off + r] = 0.0;
+        }
       }
     };
     auto boundaries = [&]() {
@@ -999,10 +1054,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       __syncthreads();  // @phase 1
       save(1, L.X0);
       // Orig := X0
-      for (int w = tid; w < nc * per; w += NT) {
-        const int cl = w / per, r = w - cl * per;
+      for (int cl = 0; cl < nc; ++cl) {
         double* col = sm + size_t(A.stride) * cl;
-        col[L.O + r] = col[L.X0 + r];
+        for (int r = tid; r < per; r += NT) col[L.O + r] = col[L.X0 + r];
       }
       __syncthreads();  // @phase 1
 
@@ -1054,10 +1108,13 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
     // cur == 0: X4 is in X0
 
     // ------------------------------------------------------------ reverse
-    for (int w = tid; w < nc * A.stride; w += NT) {
-      const int cl = w / A.stride, r = w - cl * A.stride;
-      const bool z = (r >= L.X1 && r < L.X1 + per) || (r >= L.O && r < L.O + per) || (r >= A.DB);
-      if (z) sm[w] = 0.0;
+    for (int cl = 0; cl < nc; ++cl) {
+      double* col = sm + size_t(A.stride) * cl;
+      for (int r = tid; r < per; r += NT) {
+        col[L.X1 + r] = 0.0;
+        col[L.O + r] = 0.0;
+      }
+      for (int r = A.DB + tid; r < A.stride; r += NT) col[r] = 0.0;
     }
     __syncthreads();  // @phase 0
     // scatter^T (advance_vertical.f90:163-217 and the heating line)
@@ -1116,21 +1173,16 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       }
     }
     __syncthreads();  // @phase 7
-    for (int w = tid; w < nc * per; w += NT) {
-      const int cl = w / per, r = w - cl * per;
-      double* col = sm + size_t(A.stride) * cl;
-      col[L.O + r] += col[L.X1 + r];
-      col[L.X1 + r] = 0.0;
-    }
+    fold(L.O, L.X1);
     __syncthreads();  // @phase 7
 
     const double wk[4] = {1.0, 2.0, 2.0, 1.0};
     const double ck[3] = {0.5, 0.5, 1.0};
     for (int k = 3; k >= 0; --k) {
       load(1 + k, L.X0);
-      for (int w = tid; w < nc * NSTENCIL * (nA + 2); w += NT) {
-        const int cl = w / (NSTENCIL * (nA + 2)), r = w - cl * (NSTENCIL * (nA + 2));
-        sm[size_t(A.stride) * cl + A.DB + r] = 0.0;
+      for (int cl = 0; cl < nc; ++cl) {
+        double* db = sm + size_t(A.stride) * cl + A.DB;
+        for (int r = tid; r < NSTENCIL * (nA + 2); r += NT) db[r] = 0.0;
       }
       __syncthreads();  // @phase 8
       if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
@@ -1140,15 +1192,13 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       }
       __syncthreads();  // @phase 8
       if (item) {
-        double kb[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) kb[f] = kbs[size_t(f) * NT];
         ColCtx c = ctx(my_cl);
         ColAdj a = adj(my_cl);
-        const double eb = rusanov_cell_adjoint(c, a, my_i, prm, dt, eddy, ivup, kb);
+        const double eb = cell_adjoint_species(c, a, my_i, prm, dt, eddy, kbs, NT);
+        cell_adjoint_rest(c, a, my_i, dt, ivup, kbs, NT);
         // K = New - state: the state's own -K
 #pragma unroll
-        for (int f = 0; f < NF; ++f) a.add(f, my_i, -kb[f]);
+        for (int f = 0; f < NF; ++f) a.add(f, my_i, -kbs[size_t(f) * NT]);
         if (B.eddy && !sfrozen[my_cl]) B.eddy[gidx(0, my_i + 1, my_cl)] += eb;
       }
       __syncthreads();  // @phase 9
@@ -1168,19 +1218,13 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
             kbs[size_t(f) * NT] = wk[k - 1] * acc[size_t(f) * NT] + ck[k - 1] * a.x(f, my_i);
         }
         __syncthreads();  // @phase 7
-        for (int w = tid; w < nc * per; w += NT) {
-          const int cl = w / per, r = w - cl * per;
-          double* col = sm + size_t(A.stride) * cl;
-          col[L.O + r] += col[L.X1 + r];
-          col[L.X1 + r] = 0.0;
-        }
+        fold(L.O, L.X1);
         __syncthreads();  // @phase 7
       } else {
         // X0 is also Orig
-        for (int w = tid; w < nc * per; w += NT) {
-          const int cl = w / per, r = w - cl * per;
+        for (int cl = 0; cl < nc; ++cl) {
           double* col = sm + size_t(A.stride) * cl;
-          col[L.X1 + r] += col[L.O + r];
+          for (int r = tid; r < per; r += NT) col[L.X1 + r] += col[L.O + r];
         }
         __syncthreads();  // @phase 7
         boundaries_adjoint(0);  // the first boundary pass: pre-boundary values are the gathered ones
