@@ -27,7 +27,7 @@ namespace gv {
 
 struct AdjLayout {
   Layout L;  // X0: the state; X1: its adjoint; O: the adjoint of Orig
-  int DB, CMB, GMB, TUB, MMB, stride;
+  int DB, CMB, GMB, TUB, MMB, LC, stride;
 };
 
 __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
@@ -40,6 +40,7 @@ __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
   A.GMB = o; o += G;
   A.TUB = o; o += G;
   A.MMB = o; o += 4;  // MeanMajorMass at cells -1, 0; the heating-factor sum
+  A.LC = o;  o += (NSTENCIL * (nAlts + 2) + 7) / 8;  // limiter branch per slope, one byte each
   A.stride = o;
   return A;
 }
@@ -81,32 +82,19 @@ struct AParams {
 };
 
 // ---------------------------------------------------------------- helpers
-// Adjoint of limiter_mc: (ub, db) from the output adjoint ob, on the branch
-// limiter_mc takes for (u, d).
-__device__ __forceinline__ void limiter_mc_adjoint(double u, double d, double beta, double ob, double& ub,
-                                                   double& db) {
-  ub = 0.0;
-  db = 0.0;
+// The branch of limiter_mc (ModLimiter.f90:16-36) at (u, d) that its
+// derivative follows: 0 a zero slope, 1 the slope is beta u, 2 it is beta d,
+// 3 it is the mean (u + d) / 2 (ties go to the first candidate of the
+// forward's min / max).  The slope's adjoint ob then gives u the adjoint
+// beta ob (1) or ob / 2 (3), and d beta ob (2) or ob / 2 (3).
+__device__ __forceinline__ int limiter_mc_branch(double u, double d, double beta) {
   const double bu = beta * u, bd = beta * d, av = (u + d) * 0.5;
   if (u > 0.0) {
-    if (d > 0.0) {
-      const double m = fmin(bu, bd);
-      if (m <= av) {
-        if (bu <= bd) ub = beta * ob; else db = beta * ob;
-      } else {
-        ub = 0.5 * ob;
-        db = 0.5 * ob;
-      }
-    }
-  } else if (d < 0.0) {
-    const double m = fmax(bu, bd);
-    if (m >= av) {
-      if (bu >= bd) ub = beta * ob; else db = beta * ob;
-    } else {
-      ub = 0.5 * ob;
-      db = 0.5 * ob;
-    }
+    if (d > 0.0) return (fmin(bu, bd) <= av) ? ((bu <= bd) ? 1 : 2) : 3;
+    return 0;
   }
+  if (d < 0.0) return (fmax(bu, bd) >= av) ? ((bu >= bd) ? 1 : 2) : 3;
+  return 0;
 }
 
 // Per-column view of the adjoint arrays in shared memory.
@@ -120,6 +108,7 @@ struct ColAdj {
   double* gmb;   // Gamma adjoint
   double* tub;   // TempUnit adjoint
   double* mmb;   // MeanMajorMass(-1), MeanMajorMass(0), heating-factor sum
+  uint8_t* lc;   // limiter branch of each slope [f*(nAlts+2) + cell] (limiter_mc_branch)
   int G, nA;
 
   __device__ __forceinline__ double& x(int f, int i) const { return xb[f * G + i + 1]; }
@@ -778,8 +767,34 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
   a.add(F_VU, i, VUb);
 }
 
-// Adjoint of the limited slopes of cell i (interior: 4th-order form; cells 0
-// and nAlts+1: 2nd-order form) into the state adjoint.
+// The limited slopes of cell i (interior: 4th-order form; cells 0 and
+// nAlts+1: 2nd-order form), as rusanov_slopes_interior / _end form them,
+// with each slope's limiter branch recorded for slopes_adjoint.
+__device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, int i, double beta) {
+  const int nA = c.L.nAlts;
+  if (i == 0 || i == nA + 1) {
+    const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+    for (int f = 0; f < NSTENCIL; ++f) {
+      const double* v = &c.col[c.xo + f * c.L.G + 1];
+      const double u = (v[i + 1] - v[i]) * iu, d = (v[i] - v[i - 1]) * id;
+      c.dl(f, i) = limiter_mc(u, d, beta);
+      a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(u, d, beta));
+    }
+  } else {
+    const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+#pragma unroll 3
+    for (int f = 0; f < NSTENCIL; ++f) {
+      const double* v = &c.col[c.xo + f * c.L.G + 1];
+      const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+      const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
+      c.dl(f, i) = limiter_mc(up, dn, beta);
+      a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(up, dn, beta));
+    }
+  }
+}
+
+// Adjoint of the limited slopes of cell i into the state adjoint, on the
+// branches slopes_with_branches recorded.
 __device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, double beta) {
   const int nA = c.L.nAlts;
   const bool end = (i == 0 || i == nA + 1);
@@ -787,19 +802,10 @@ __device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, d
   const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
   for (int f = 0; f < NSTENCIL; ++f) {
     const double ob = a.db[f * (nA + 2) + i];
-    if (ob == 0.0) continue;
-    const double* v = &c.col[c.xo + f * c.L.G + 1];
-    double u, d;
-    if (end) {
-      u = (v[i + 1] - v[i]) * iu;
-      d = (v[i] - v[i - 1]) * id;
-    } else {
-      u = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-      d = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-    }
-    double ub, dbv;
-    limiter_mc_adjoint(u, d, beta, ob, ub, dbv);
-    if (ub == 0.0 && dbv == 0.0) continue;
+    const int br = a.lc[f * (nA + 2) + i];
+    if (ob == 0.0 || br == 0) continue;
+    const double ub = (br == 1) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
+    const double dbv = (br == 2) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
     if (end) {
       a.add(f, i + 1, iu * ub);
       a.add(f, i, -iu * ub + id * dbv);
@@ -880,6 +886,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       a.gmb = col + A.GMB;
       a.tub = col + A.TUB;
       a.mmb = col + A.MMB;
+      a.lc = reinterpret_cast<uint8_t*>(col + A.LC);
       a.G = G;
       a.nA = nA;
       return a;
@@ -1185,10 +1192,10 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         for (int r = tid; r < NSTENCIL * (nA + 2); r += NT) db[r] = 0.0;
       }
       __syncthreads();  // @phase 8
-      if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
+      if (item) slopes_with_branches(ctx(my_cl), adj(my_cl), my_i, prm.beta_limiter);
       for (int q = tid - nitems; q < nc * 2; q += NT) {
         if (q < 0) continue;
-        rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+        slopes_with_branches(ctx(q >> 1), adj(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
       }
       __syncthreads();  // @phase 8
       if (item) {
