@@ -768,28 +768,26 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
 }
 
 // The limited slopes of cell i (interior: 4th-order form; cells 0 and
-// nAlts+1: 2nd-order form), as rusanov_slopes_interior / _end form them,
-// with each slope's limiter branch recorded for slopes_adjoint.
+// nAlts+1: 2nd-order form), as rusanov_slopes_cell forms them, with each
+// slope's limiter branch recorded for slopes_adjoint.
 __device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, int i, double beta) {
   const int nA = c.L.nAlts;
-  if (i == 0 || i == nA + 1) {
-    const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
-    for (int f = 0; f < NSTENCIL; ++f) {
-      const double* v = &c.col[c.xo + f * c.L.G + 1];
-      const double u = (v[i + 1] - v[i]) * iu, d = (v[i] - v[i - 1]) * id;
-      c.dl(f, i) = limiter_mc(u, d, beta);
-      a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(u, d, beta));
-    }
-  } else {
-    const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+  const bool end = (i == 0 || i == nA + 1);
+  const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
+  const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
 #pragma unroll 3
-    for (int f = 0; f < NSTENCIL; ++f) {
-      const double* v = &c.col[c.xo + f * c.L.G + 1];
-      const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-      const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-      c.dl(f, i) = limiter_mc(up, dn, beta);
-      a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(up, dn, beta));
+  for (int f = 0; f < NSTENCIL; ++f) {
+    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    double u, d;
+    if (end) {
+      u = (v[i + 1] - v[i]) * cu;
+      d = (v[i] - v[i - 1]) * cd;
+    } else {
+      u = cu * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+      d = cd * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
     }
+    c.dl(f, i) = limiter_mc(u, d, beta);
+    a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(u, d, beta));
   }
 }
 
@@ -798,8 +796,10 @@ __device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, in
 __device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, double beta) {
   const int nA = c.L.nAlts;
   const bool end = (i == 0 || i == nA + 1);
-  const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
-  const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
+  // end cells: u = (v[i+1] - v[i]) cu, d = (v[i] - v[i-1]) cd; interior:
+  // the 4th-order differences with the mesh factors cu, cd
+  const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
+  const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
   for (int f = 0; f < NSTENCIL; ++f) {
     const double ob = a.db[f * (nA + 2) + i];
     const int br = a.lc[f * (nA + 2) + i];
@@ -807,15 +807,15 @@ __device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, d
     const double ub = (br == 1) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
     const double dbv = (br == 2) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
     if (end) {
-      a.add(f, i + 1, iu * ub);
-      a.add(f, i, -iu * ub + id * dbv);
-      a.add(f, i - 1, -id * dbv);
+      a.add(f, i + 1, cu * ub);
+      a.add(f, i, -cu * ub + cd * dbv);
+      a.add(f, i - 1, -cd * dbv);
     } else {
-      a.add(f, i + 2, -h2u * F2 * ub);
-      a.add(f, i + 1, h2u * F1 * ub - h2d * F2 * dbv);
-      a.add(f, i, -h2u * F1 * ub + h2d * F1 * dbv);
-      a.add(f, i - 1, h2u * F2 * ub - h2d * F1 * dbv);
-      a.add(f, i - 2, h2d * F2 * dbv);
+      a.add(f, i + 2, -cu * F2 * ub);
+      a.add(f, i + 1, cu * F1 * ub - cd * F2 * dbv);
+      a.add(f, i, -cu * F1 * ub + cd * F1 * dbv);
+      a.add(f, i - 1, cu * F2 * ub - cd * F1 * dbv);
+      a.add(f, i - 2, cd * F2 * dbv);
     }
   }
 }
@@ -1069,10 +1069,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
 
       // ------------------------------------------------------------ forward
       for (int k = 0; k < 4; ++k) {
-        if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
-        for (int q = tid - nitems; q < nc * 2; q += NT) {
-          if (q < 0) continue;
-          rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+        for (int j = tid; j < nc * (nA + 2); j += NT) {
+          const int cl = j / (nA + 2), i = j - cl * (nA + 2);
+          rusanov_slopes_cell(ctx(cl), i, prm.beta_limiter);
         }
         __syncthreads();  // @phase 2
         const int nxo = cur ? L.X0 : L.X1;
@@ -1192,10 +1191,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         for (int r = tid; r < NSTENCIL * (nA + 2); r += NT) db[r] = 0.0;
       }
       __syncthreads();  // @phase 8
-      if (item) slopes_with_branches(ctx(my_cl), adj(my_cl), my_i, prm.beta_limiter);
-      for (int q = tid - nitems; q < nc * 2; q += NT) {
-        if (q < 0) continue;
-        slopes_with_branches(ctx(q >> 1), adj(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+      for (int j = tid; j < nc * (nA + 2); j += NT) {
+        const int cl = j / (nA + 2), i = j - cl * (nA + 2);
+        slopes_with_branches(ctx(cl), adj(cl), i, prm.beta_limiter);
       }
       __syncthreads();  // @phase 8
       if (item) {
@@ -1209,10 +1207,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         if (B.eddy && !sfrozen[my_cl]) B.eddy[gidx(0, my_i + 1, my_cl)] += eb;
       }
       __syncthreads();  // @phase 9
-      if (item) slopes_adjoint(ctx(my_cl), adj(my_cl), my_i, prm.beta_limiter);
-      for (int q = tid - nitems; q < nc * 2; q += NT) {
-        if (q < 0) continue;
-        slopes_adjoint(ctx(q >> 1), adj(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+      for (int j = tid; j < nc * (nA + 2); j += NT) {
+        const int cl = j / (nA + 2), i = j - cl * (nA + 2);
+        slopes_adjoint(ctx(cl), adj(cl), i, prm.beta_limiter);
       }
       __syncthreads();  // @phase 10
       if (k > 0) {

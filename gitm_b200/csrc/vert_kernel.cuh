@@ -587,23 +587,26 @@ __device__ __forceinline__ void rusanov_cell(ColCtx c, int i, const GitmVertPara
 
 // Limited slopes of the 18 swept fields at cell i: the 4th-order form on
 // interior cells, the 2nd-order one on cells 0 and nAlts+1
-// (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772).
-__device__ __forceinline__ void rusanov_slopes_interior(ColCtx c, int i, double beta) {
-  const double h2u = c.g(GC_H2, i + 1), h2d = c.g(GC_H2, i);
+// (calc_facevalues_alts_rusanov, vertical_solver_rusanov.f90:745-772),
+// the choice made per field, so that a warp whose lanes hold both kinds of
+// cell diverges only over the two differences (threads over cells
+// 0..nAlts+1 of every column).
+__device__ __forceinline__ void rusanov_slopes_cell(ColCtx c, int i, double beta) {
+  const bool end = (i == 0 || i == c.L.nAlts + 1);
+  const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
+  const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
 #pragma unroll 3
   for (int f = 0; f < NSTENCIL; ++f) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
-    const double up = h2u * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-    const double dn = h2d * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-    c.dl(f, i) = limiter_mc(up, dn, beta);
-  }
-}
-
-__device__ __forceinline__ void rusanov_slopes_end(ColCtx c, int i, double beta) {
-  const double iu = c.g(GC_IDF, i + 1), id = c.g(GC_IDF, i);
-  for (int f = 0; f < NSTENCIL; ++f) {
-    const double* v = &c.col[c.xo + f * c.L.G + 1];
-    c.dl(f, i) = limiter_mc((v[i + 1] - v[i]) * iu, (v[i] - v[i - 1]) * id, beta);
+    double u, d;
+    if (end) {
+      u = (v[i + 1] - v[i]) * cu;
+      d = (v[i] - v[i - 1]) * cd;
+    } else {
+      u = cu * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
+      d = cd * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
+    }
+    c.dl(f, i) = limiter_mc(u, d, beta);
   }
 }
 
@@ -895,24 +898,19 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             ausm_prefix(c, lane);
           }
           __syncthreads();  // @phase 6
-          if (item) {
-            ColCtx c = ctx(my_cl);
+          // threads over cells 0..nAlts+1 of every column
+          for (int j = tid; j < nc * (nA + 2); j += NT) {
+            const int cl = j / (nA + 2), i = j - cl * (nA + 2);
+            ColCtx c = ctx(cl);
 #pragma unroll 4
-            for (int f = 0; f < NSLOPE_AUSM; ++f) c.dl(f, my_i) = ausm_slope(c, f, my_i, prm.beta_limiter);
-          }
-          for (int q = tid - nitems; q < nc * 2; q += NT) {
-            if (q < 0) continue;
-            ColCtx c = ctx(q >> 1);
-            const int i = (q & 1) ? nA + 1 : 0;
             for (int f = 0; f < NSLOPE_AUSM; ++f) c.dl(f, i) = ausm_slope(c, f, i, prm.beta_limiter);
           }
         } else {
-          // limited slopes of the 18 swept fields on cells 0..nAlts+1
-          if (item) rusanov_slopes_interior(ctx(my_cl), my_i, prm.beta_limiter);
-          // the two end slopes of each column
-          for (int q = tid - nitems; q < nc * 2; q += NT) {
-            if (q < 0) continue;
-            rusanov_slopes_end(ctx(q >> 1), (q & 1) ? nA + 1 : 0, prm.beta_limiter);
+          // limited slopes of the 18 swept fields on cells 0..nAlts+1,
+          // threads over the cells of every column
+          for (int j = tid; j < nc * (nA + 2); j += NT) {
+            const int cl = j / (nA + 2), i = j - cl * (nA + 2);
+            rusanov_slopes_cell(ctx(cl), i, prm.beta_limiter);
           }
         }
         __syncthreads();  // @phase 2
