@@ -46,6 +46,9 @@ SIGNATURES = {
                                    C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "gitm_vert_advance_fortran": (C.c_int, [_P, C.POINTER(abi.GitmFortranState), C.c_int, C.c_int,
                                             C.c_double, C.c_int]),
+    # include/gitm_hz.h
+    "gitm_hz_advance": (C.c_int, [_P, C.POINTER(abi.GitmHzParams), C.POINTER(abi.GitmHzBlocks), C.c_double, _P]),
+    "gitm_hz_status": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_int]),
 }
 
 

@@ -203,6 +203,48 @@ class GitmFortranState(C.Structure):
     ] + [(name, GitmFArray) for name in FORTRAN_ARRAYS]
 
 
+NSPECIES_TOTAL = 11  # GITM_NSPECIES_TOTAL: NDensityS's species extent
+
+HZ_BLOCK_FIELDS = ("rho", "temperature", "velocity", "vert_vel", "ndensity_s", "idensity_s", "temp_source",
+                   "gamma", "cmax", "ivelocity", "ivelocity_par", "latitude", "tan_latitude", "cos_latitude",
+                   "radial_distance", "inv_radial_distance", "inv_dlon_dist_gb", "inv_dlon_dist_fb",
+                   "dlon_dist_fb", "inv_dlat_dist_gb", "inv_dlat_dist_fb", "dlat_dist_fb", "grad_lon_m",
+                   "grad_lon_0", "grad_lon_p", "grad_lat_m", "grad_lat_0", "grad_lat_p")
+
+
+class GitmHzParams(C.Structure):
+    _fields_ = [
+        ("use_coriolis", C.c_int32),
+        ("use_ion_advection", C.c_int32),
+        ("use_improved_ion_advection", C.c_int32),
+        ("non_magnetic", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("omega_body", C.c_double),
+        ("beta_limiter", C.c_double),
+    ]
+
+
+def default_hz_params(**overrides) -> GitmHzParams:
+    """Reference defaults (ModInputs.f90: UseCoriolis, UseIonAdvection,
+    UseImprovedIonAdvection true; BetaLimiter 2; OmegaBodyInput 2 pi / day);
+    Earth is magnetic (NonMagnetic false)."""
+    p = GitmHzParams()
+    p.use_coriolis = 1
+    p.use_ion_advection = 1
+    p.use_improved_ion_advection = 1
+    p.non_magnetic = 0
+    p.omega_body = 2.0 * 3.141592653589793 / (24.0 * 3600.0)
+    p.beta_limiter = 2.0
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+class GitmHzBlocks(C.Structure):
+    _fields_ = [("n_lons", C.c_int32), ("n_lats", C.c_int32), ("n_alts", C.c_int32), ("n_blocks", C.c_int32)] + \
+        [(name, _dp) for name in HZ_BLOCK_FIELDS]
+
+
 def dptr(addr: int):
     """A ctypes double* from an integer address (0 -> NULL)."""
     return C.cast(C.c_void_p(addr), _dp) if addr else _dp()

@@ -21,9 +21,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgitmvert.so")
-SOURCES = ["gitm_vert.cu", "vert_adjoint.cu"]
-DEPS = ["gitm_vert.cu", "vert_adjoint.cu", "vert_instance.cu", "vert_instances.h", "vert_kernel.cuh",
-        "vert_ausm.cuh", "vert_adjoint.cuh", "vert_common.cuh"]
+SOURCES = ["gitm_vert.cu", "vert_adjoint.cu", "hz_kernel.cu"]
+DEPS = ["gitm_vert.cu", "vert_adjoint.cu", "hz_kernel.cu", "vert_instance.cu", "vert_instances.h", "vert_kernel.cuh",
+        "vert_ausm.cuh", "vert_adjoint.cuh", "vert_common.cuh", "vert_hz.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -59,6 +59,7 @@ def stale() -> bool:
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, d) for d in DEPS]
     deps.append(os.path.join(HERE, "..", "include", "gitm_vert.h"))
+    deps.append(os.path.join(HERE, "..", "include", "gitm_hz.h"))
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

@@ -20,6 +20,7 @@
 #include "vert_kernel.cuh"
 #include "vert_adjoint.cuh"
 #include "vert_instances.h"
+#include "vert_hz.cuh"
 
 using namespace gv;
 
@@ -41,6 +42,11 @@ struct GitmVertCtx {
   GitmVertPlan* host_plan = nullptr;
   std::vector<uint64_t> host_plan_key;
   std::vector<cudaEvent_t> events;  // chunk hand-offs between the host path's streams
+  // gitm_hz_advance: one status word per block, the stream of the last call
+  uint32_t* hz_status = nullptr;
+  int64_t hz_status_n = 0;
+  int64_t hz_blocks = 0;
+  cudaStream_t hz_stream = nullptr;
 };
 
 static int arena_reserve(GitmVertCtx* ctx, size_t bytes);
@@ -340,6 +346,7 @@ int gitm_vert_destroy(GitmVertCtx* ctx) {
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   cudaFree(ctx->arena);
   cudaFree(ctx->d_scalar);
+  cudaFree(ctx->hz_status);
   for (cudaStream_t& st : ctx->streams)
     if (st) cudaStreamDestroy(st);
   delete ctx;
@@ -1665,5 +1672,83 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   const int grid = std::min(n_tiles, kNoAllocSlots);
   CUDA_TRY(ctx, cudaLaunchKernel(kernel_for(0, GITM_SOLVER_RUSANOV, kNoAllocThreads), dim3(grid),
                                  dim3(kNoAllocThreads), args, smem, st));
+  return GITM_OK;
+}
+
+// ------------------------------------------------------------------ horizontal advance
+// gitm_hz_advance / gitm_hz_status (include/gitm_hz.h): advance_horizontal
+// (advance_horizontal.f90:58-924) for every block of GITM's own device
+// arrays; the kernel is in hz_kernel.cu.
+extern "C" int gitm_hz_advance(GitmVertCtx* ctx, const GitmHzParams* params, const GitmHzBlocks* blocks, double dt,
+                               void* stream) {
+  if (!ctx || !params || !blocks) return set_err(ctx, GITM_ERR_ARG, "bad arguments");
+  const GitmHzBlocks& b = *blocks;
+  if (b.n_lons < 1 || b.n_lats < 1 || b.n_alts < 1 || b.n_blocks < 0)
+    return set_err(ctx, GITM_ERR_ARG, "bad block shape %d x %d x %d, %d blocks", b.n_lons, b.n_lats, b.n_alts,
+                   b.n_blocks);
+  if (hz_threads(b.n_lons, b.n_lats) == 0)
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "blocks of %d x %d cells: at most 256 cells per block are built",
+                   b.n_lons, b.n_lats);
+  if (int64_t(b.n_blocks) * b.n_alts > int64_t(0x7fffffff))
+    return set_err(ctx, GITM_ERR_ARG, "too many (block, altitude) planes");
+  if (!(dt > 0.0)) return set_err(ctx, GITM_ERR_ARG, "dt must be > 0");
+  if (!(params->beta_limiter >= 1.0 && params->beta_limiter <= 2.0))
+    return set_err(ctx, GITM_ERR_ARG, "beta_limiter %g outside [1, 2]", params->beta_limiter);
+  const bool div = params->use_ion_advection && params->use_improved_ion_advection;
+  const void* req[] = {b.rho, b.temperature, b.velocity, b.vert_vel, b.ndensity_s, b.idensity_s, b.gamma, b.cmax,
+                       b.ivelocity, b.latitude, b.tan_latitude, b.cos_latitude, b.radial_distance,
+                       b.inv_radial_distance, b.inv_dlon_dist_gb, b.inv_dlon_dist_fb, b.dlon_dist_fb,
+                       b.inv_dlat_dist_gb, b.inv_dlat_dist_fb, b.dlat_dist_fb};
+  for (const void* p : req)
+    if (!p || !is_device_ptr(p)) return set_err(ctx, GITM_ERR_ARG, "the block arrays must be non-NULL device pointers");
+  if (div) {
+    const void* dreq[] = {params->non_magnetic ? (const void*)b.ivelocity : (const void*)b.ivelocity_par,
+                          b.grad_lon_m, b.grad_lon_0, b.grad_lon_p, b.grad_lat_m, b.grad_lat_0, b.grad_lat_p};
+    for (const void* p : dreq)
+      if (!p || !is_device_ptr(p))
+        return set_err(ctx, GITM_ERR_ARG, "the ion-divergence term needs IVelocityPar and the GradLon/GradLat arrays");
+  }
+  if (!is_device_ptr(b.temp_source)) return set_err(ctx, GITM_ERR_ARG, "temp_source must be a device pointer");
+  if (b.n_blocks == 0) return GITM_OK;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (ctx->hz_status_n < b.n_blocks) {
+    cudaFree(ctx->hz_status);
+    ctx->hz_status = nullptr;
+    ctx->hz_status_n = 0;
+    if (cudaMalloc(&ctx->hz_status, size_t(b.n_blocks) * sizeof(uint32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, GITM_ERR_NOMEM, "cannot allocate the block status words");
+    }
+    ctx->hz_status_n = b.n_blocks;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(ctx, cudaMemsetAsync(ctx->hz_status, 0, size_t(b.n_blocks) * sizeof(uint32_t), st));
+  const size_t smem = hz_smem_bytes(b.n_lons, b.n_lats);
+  if (smem > ctx->max_smem) return set_err(ctx, GITM_ERR_UNSUPPORTED, "block plane needs %zu bytes of shared memory", smem);
+  cudaError_t e = hz_launch(*params, b, dt, ctx->hz_status, st);
+  if (e != cudaSuccess) return set_err(ctx, GITM_ERR_CUDA, "hz launch: %s", cudaGetErrorString(e));
+  ctx->hz_blocks = b.n_blocks;
+  ctx->hz_stream = st;
+  return GITM_OK;
+}
+
+extern "C" int gitm_hz_status(GitmVertCtx* ctx, uint32_t* or_out, int64_t* n_bad, int clear) {
+  if (!ctx) return GITM_ERR_ARG;
+  if (or_out) *or_out = 0;
+  if (n_bad) *n_bad = 0;
+  if (ctx->hz_blocks == 0) return GITM_OK;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->hz_stream));
+  std::vector<uint32_t> w(size_t(ctx->hz_blocks));
+  CUDA_TRY(ctx, cudaMemcpy(w.data(), ctx->hz_status, w.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  uint32_t acc = 0;
+  int64_t nb = 0;
+  for (uint32_t x : w) {
+    acc |= x;
+    nb += (x != 0);
+  }
+  if (or_out) *or_out = acc;
+  if (n_bad) *n_bad = nb;
+  if (clear) CUDA_TRY(ctx, cudaMemset(ctx->hz_status, 0, w.size() * sizeof(uint32_t)));
   return GITM_OK;
 }

@@ -1,0 +1,424 @@
+// hz_kernel.cu -- the horizontal advance (advance_horizontal.f90:58-1034) on
+// the GPU: gitm_hz_advance's kernel, in its own translation unit.
+//
+// One CTA per (block, altitude) plane.  The plane's swept fields (Rho,
+// Temperature, Velocity, the six NDensityS and VerticalVelocity, the advected
+// IDensityS: 19 fields) and its grid metrics are loaded with their two ghost
+// rings from GITM's own Fortran-layout arrays (a plane of one field is
+// contiguous there, longitude fastest) into shared memory; one thread per
+// interior cell runs the four RK stages of :168-345, each stage the whole
+// horizontal_solver (:535-818) at the thread's cell: for every field the
+// limited slopes of calc_facevalues_lons / _lats (:928-1034) at the cell and
+// its two neighbours, the face values, the Rusanov gradient and diffusion
+// (calc_rusanov_lons / _lats, :821-922), then the cell's equations.  The
+// ghost rings keep their values through the stages, as in the reference.
+// The store phase writes the interior cells back with the stores of
+// :346-421 and, with UseImprovedIonAdvection, the parallel ion-velocity
+// divergence of :423-517 (UAM_Gradient, gradient.f90:4-104) at the cell,
+// which reads only IVelocityPar and the grid; the CTA of the first and last
+// altitude also rewrite the electron sum of the ghost planes.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/gitm_hz.h"
+#include "vert_common.cuh"
+#include "vert_hz.cuh"
+
+namespace gv {
+
+namespace {
+
+constexpr int HZ_NSW = 5 + 2 * NS + NADV;  // swept fields
+constexpr int NI_ALL = GITM_NIONS - 1;     // ions without the electrons
+constexpr int HF_R = 0, HF_T = 1, HF_V = 2, HF_N = 5, HF_W = 5 + NS, HF_I = 5 + 2 * NS;
+constexpr int HZ_NGP = 6;   // metric planes with ghost rings: IFB, DFB lon; IFB, DFB lat; cMax E, N
+constexpr int HZ_NGC = 7;   // metric values at interior cells: InvD*Dist_GB lon, lat; Gamma; InvR; R; IVel E, N
+constexpr double F1 = 0.6250000;  // Factor1, advance_horizontal.f90:939
+constexpr double F2 = 0.0416667;  // Factor2, advance_horizontal.f90:940
+
+// Shared-memory plan of one plane: P cells with ghosts, C interior cells.
+struct HzLayout {
+  int P, C;
+  int S, O, K, G, GC, stride;
+};
+
+__host__ __device__ inline HzLayout hz_layout(int nLons, int nLats) {
+  HzLayout L;
+  L.P = (nLons + 4) * (nLats + 4);
+  L.C = nLons * nLats;
+  int o = 0;
+  L.S = o;  o += HZ_NSW * L.P;
+  L.O = o;  o += HZ_NSW * L.C;
+  L.K = o;  o += HZ_NSW * L.C;  // the stage's New - state of every field
+  L.G = o;  o += HZ_NGP * L.P;
+  L.GC = o; o += HZ_NGC * L.C;
+  L.stride = o;
+  return L;
+}
+
+// Limiter_mc (ModLimiter.f90:16-36)
+__device__ __forceinline__ double hz_limiter(double u, double d, double beta) {
+  if (u > 0.0) {
+    if (d > 0.0) return fmin(fmin(beta * u, beta * d), (u + d) * 0.5);
+    return 0.0;
+  }
+  if (d < 0.0) return fmax(fmax(beta * u, beta * d), (u + d) * 0.5);
+  return 0.0;
+}
+
+// The limited slope of line cell q (0 .. n+1) as calc_facevalues_lons /
+// _lats form it: the 4th-order differences, with the 2nd-order one on the
+// outer side of cells 0 and n+1.  V(q) = V[(q+1)*s], IF(q) = IF[(q+1)*s].
+__device__ __forceinline__ double hz_slope(const double* V, const double* IF, int s, int q, int n,
+                                           double beta) {
+  auto v = [&](int x) { return V[(x + 1) * s]; };
+  auto f = [&](int x) { return IF[(x + 1) * s]; };
+  double up, dn;
+  if (q == n + 1) {
+    up = (v(q + 1) - v(q)) * f(q + 1);
+  } else {
+    const double h = f(q + 1) * 2;
+    up = h * (F1 * (v(q + 1) - v(q)) - F2 * (v(q + 2) - v(q - 1)));
+  }
+  if (q == 0) {
+    dn = (v(q) - v(q - 1)) * f(q);
+  } else {
+    const double h = f(q) * 2;
+    dn = h * (F1 * (v(q) - v(q - 1)) - F2 * (v(q + 1) - v(q - 2)));
+  }
+  return hz_limiter(up, dn, beta);
+}
+
+// calc_rusanov_lons / _lats at line cell p (1..n): the gradient and the
+// Rusanov diffusion from the face values of faces p and p+1.
+__device__ __forceinline__ void hz_line(const double* V, const double* IF, const double* DF, const double* CM,
+                                        int s, int p, int n, double invd, double beta, double& grad,
+                                        double& diff) {
+  const double sm = hz_slope(V, IF, s, p - 1, n, beta);
+  const double s0 = hz_slope(V, IF, s, p, n, beta);
+  const double sp = hz_slope(V, IF, s, p + 1, n, beta);
+  const double vm = V[p * s], v0 = V[(p + 1) * s], vp = V[(p + 2) * s];
+  const double d0 = DF[(p + 1) * s], d1 = DF[(p + 2) * s];
+  const double W0 = vm + 0.5 * sm * d0;  // VarLeft(p)
+  const double E0 = v0 - 0.5 * s0 * d0;  // VarRight(p)
+  const double W1 = v0 + 0.5 * s0 * d1;  // VarLeft(p+1)
+  const double E1 = vp - 0.5 * sp * d1;  // VarRight(p+1)
+  grad = 0.5 * (W1 + E1 - W0 - E0) * invd;
+  const double c0 = 0.5 * fmax(CM[p * s], CM[(p + 1) * s]) * (E0 - W0);
+  const double c1 = 0.5 * fmax(CM[(p + 1) * s], CM[(p + 2) * s]) * (E1 - W1);
+  diff = (c1 - c0) * invd;
+}
+
+struct HzArgs {
+  GitmHzParams prm;
+  GitmHzBlocks b;
+  double dt;
+  uint32_t* status;  // one word per block
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) hz_step_kernel(const HzArgs A) {
+  extern __shared__ double sm[];
+  const GitmHzBlocks& B = A.b;
+  const GitmHzParams& prm = A.prm;
+  const int nl = B.n_lons, nt = B.n_lats, na = B.n_alts;
+  const int NI = nl + 4, NJ = nt + 4, NK = na + 4;
+  const int64_t P = int64_t(NI) * NJ, V = P * NK;
+  const int k = blockIdx.x % na + 1;  // Fortran altitude of this plane
+  const int b = blockIdx.x / na;
+  const int tid = threadIdx.x;
+  const HzLayout L = hz_layout(nl, nt);
+  const double dt = A.dt;
+  // first element of plane k of field f of a block array with nf fields
+  auto plane = [&](const double* a, int f, int nf) -> const double* {
+    return a + ((int64_t(b) * nf + f) * NK + (k + 1)) * P;
+  };
+  auto lat1 = [&](const double* a, int j) { return a[int64_t(b) * NJ + (j + 1)]; };
+
+  // ---------------------------------------------------------------- load
+  double* S = sm + L.S;
+  double* O = sm + L.O;
+  double* Kc = sm + L.K;
+  double* GP = sm + L.G;
+  double* GC = sm + L.GC;
+  auto src_of = [&](int f) -> const double* {
+    if (f == HF_R) return plane(B.rho, 0, 1);
+    if (f == HF_T) return plane(B.temperature, 0, 1);
+    if (f < HF_N) return plane(B.velocity, f - HF_V, 3);
+    if (f < HF_W) return plane(B.ndensity_s, f - HF_N, GITM_NSPECIES_TOTAL);
+    if (f < HF_I) return plane(B.vert_vel, f - HF_W, NS);
+    return plane(B.idensity_s, f - HF_I, GITM_NIONS);
+  };
+  for (int f = 0; f < HZ_NSW; ++f) {
+    const double* src = src_of(f);
+    for (int c = tid; c < P; c += NT) S[f * P + c] = src[c];
+  }
+  {
+    const double* gsrc[HZ_NGP] = {plane(B.inv_dlon_dist_fb, 0, 1), plane(B.dlon_dist_fb, 0, 1),
+                                  plane(B.inv_dlat_dist_fb, 0, 1), plane(B.dlat_dist_fb, 0, 1),
+                                  plane(B.cmax, 0, 3), plane(B.cmax, 1, 3)};
+    for (int g = 0; g < HZ_NGP; ++g)
+      for (int c = tid; c < P; c += NT) GP[g * P + c] = gsrc[g][c];
+  }
+  const bool cell = tid < L.C;
+  const int ci = cell ? tid % nl + 1 : 1, cj = cell ? tid / nl + 1 : 1;  // Fortran (iLon, iLat)
+  const int pc = (cj + 1) * NI + (ci + 1);                                // plane index of the cell
+  if (cell) {
+    GC[0 * L.C + tid] = plane(B.inv_dlon_dist_gb, 0, 1)[pc];
+    GC[1 * L.C + tid] = plane(B.inv_dlat_dist_gb, 0, 1)[pc];
+    GC[2 * L.C + tid] = plane(B.gamma, 0, 1)[pc];
+    GC[3 * L.C + tid] = plane(B.inv_radial_distance, 0, 1)[pc];
+    GC[4 * L.C + tid] = plane(B.radial_distance, 0, 1)[pc];
+    GC[5 * L.C + tid] = plane(B.ivelocity, 0, 3)[pc];
+    GC[6 * L.C + tid] = plane(B.ivelocity, 1, 3)[pc];
+  }
+  __syncthreads();
+  if (cell)
+    for (int f = 0; f < HZ_NSW; ++f) O[f * L.C + tid] = S[f * P + pc];
+
+  // per-cell constants of the equations (:680-686)
+  double SinLat = 0.0, CosLat = 0.0, TanLat = 0.0;
+  if (cell) {
+    SinLat = sin(lat1(B.latitude, cj));
+    CosLat = lat1(B.cos_latitude, cj);
+    TanLat = lat1(B.tan_latitude, cj);
+  }
+  const double CoriolisSin = SinLat * 2 * prm.omega_body;
+  const double CoriolisCos = CosLat * 2 * prm.omega_body;
+  const double CentrifugalParameter = (prm.omega_body * prm.omega_body) * CosLat * SinLat;
+  const double beta = prm.beta_limiter;
+  const double* IFlo = GP + 0 * P;
+  const double* DFlo = GP + 1 * P;
+  const double* IFla = GP + 2 * P;
+  const double* DFla = GP + 3 * P;
+  const double* CMe = GP + 4 * P;
+  const double* CMn = GP + 5 * P;
+
+  // the Rusanov gradient / diffusion of field f at the cell along lon, lat
+  auto lon_of = [&](int f, double& g, double& d) {
+    const int row = (cj + 1) * NI;
+    hz_line(S + f * P + row, IFlo + row, DFlo + row, CMe + row, 1, ci, nl, GC[0 * L.C + tid], beta, g, d);
+  };
+  auto lat_of = [&](int f, double& g, double& d) {
+    const int col = ci + 1;
+    hz_line(S + f * P + col, IFla + col, DFla + col, CMn + col, NI, cj, nt, GC[1 * L.C + tid], beta, g, d);
+  };
+
+  double acc[HZ_NSW];
+  __syncthreads();
+
+  // ---------------------------------------------------------------- RK4
+  for (int st = 0; st < 4; ++st) {
+    auto kv = [&](int f) -> double& { return Kc[f * L.C + tid]; };
+    if (cell) {
+      const double InvR = GC[3 * L.C + tid];
+      const double R = S[HF_R * P + pc], T = S[HF_T * P + pc];
+      const double VE = S[(HF_V + 0) * P + pc], VN = S[(HF_V + 1) * P + pc], VU = S[(HF_V + 2) * P + pc];
+      double gLoR, dLoR, gLaR, dLaR, gLoT, dLoT, gLaT, dLaT;
+      double gLoE, dLoE, gLaE, dLaE, gLoN, dLoN, gLaN, dLaN, gLoU, dLoU, gLaU, dLaU;
+      lon_of(HF_R, gLoR, dLoR);
+      lat_of(HF_R, gLaR, dLaR);
+      lon_of(HF_T, gLoT, dLoT);
+      lat_of(HF_T, gLaT, dLaT);
+      lon_of(HF_V + 0, gLoE, dLoE);
+      lat_of(HF_V + 0, gLaE, dLaE);
+      lon_of(HF_V + 1, gLoN, dLoN);
+      lat_of(HF_V + 1, gLaN, dLaN);
+      lon_of(HF_V + 2, gLoU, dLoU);
+      lat_of(HF_V + 2, gLaU, dLaU);
+      // DivVel_C (:614-617)
+      const double DivVel = gLaN + gLoE - TanLat * VN * InvR;
+      // :688-694
+      kv(HF_R) = (R - dt * (R * DivVel + gLaR * VN + gLoR * VE) + dt * (dLoR + dLaR)) - R;
+      // :749-759, :765-777, :785-790 and the Coriolis terms of :803-813
+      double nE = VE - dt * (VN * gLaE + VE * gLoE + VE * (VU - TanLat * VN) * InvR + gLoT + gLoR * T / R) +
+                  dt * (dLoE + dLaE);
+      double nN = VN - dt * (VN * gLaN + VE * gLoN + (VN * VU + TanLat * (VE * VE)) * InvR + gLaT + gLaR * T / R) +
+                  dt * (dLoN + dLaN);
+      const double nU = VU - dt * (VN * gLaU + VE * gLoU) + dt * (dLoU + dLaU);
+      if (prm.use_coriolis) {
+        nE = nE + dt * (+CoriolisSin * VN - CoriolisCos * VU);
+        nN = nN - dt * (CentrifugalParameter * GC[4 * L.C + tid] + CoriolisSin * VE);
+      }
+      kv(HF_V + 0) = nE - VE;
+      kv(HF_V + 1) = nN - VN;
+      kv(HF_V + 2) = nU - VU;
+      // :817-823
+      kv(HF_T) = (T - dt * ((GC[2 * L.C + tid] - 1) * T * DivVel + gLaT * VN + gLoT * VE) + dt * (dLoT + dLaT)) - T;
+      // species continuity (:696-703) and vertical winds (:794-801)
+#pragma unroll 1
+      for (int s = 0; s < NS; ++s) {
+        double gLo, dLo, gLa, dLa;
+        lon_of(HF_N + s, gLo, dLo);
+        lat_of(HF_N + s, gLa, dLa);
+        const double x = S[(HF_N + s) * P + pc];
+        kv(HF_N + s) = (x - dt * (x * DivVel + gLa * VN + gLo * VE) + dt * (dLo + dLa)) - x;
+        lon_of(HF_W + s, gLo, dLo);
+        lat_of(HF_W + s, gLa, dLa);
+        const double w = S[(HF_W + s) * P + pc];
+        kv(HF_W + s) = (w - dt * (VN * gLa + VE * gLo) + dt * (dLa + dLo)) - w;
+      }
+      // advected ions (:719-736)
+#pragma unroll 1
+      for (int s = 0; s < NADV; ++s) {
+        double gLo, dLo, gLa, dLa;
+        lon_of(HF_I + s, gLo, dLo);
+        lat_of(HF_I + s, gLa, dLa);
+        const double x = S[(HF_I + s) * P + pc];
+        kv(HF_I + s) =
+            (x - dt * (+gLa * GC[6 * L.C + tid] + gLo * GC[5 * L.C + tid]) + dt * (dLo + dLa)) - x;
+      }
+    }
+    __syncthreads();  // every read of this stage's state is done
+    if (cell) {
+#pragma unroll
+      for (int f = 0; f < HZ_NSW; ++f) {
+        const double o = O[f * L.C + tid];
+        const double kf = Kc[f * L.C + tid];
+        double nx;
+        if (st == 0) {
+          acc[f] = kf;
+          nx = 0.5 * kf + o;
+        } else if (st == 1) {
+          acc[f] = acc[f] + 2.0 * kf;
+          nx = 0.5 * kf + o;
+        } else if (st == 2) {
+          acc[f] = acc[f] + 2.0 * kf;
+          nx = kf + o;
+        } else {
+          acc[f] = acc[f] + kf;
+          nx = o + (1.0 / 6.0) * acc[f];
+        }
+        S[f * P + pc] = nx;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---------------------------------------------------------------- store
+  auto out = [&](double* a, int f, int nf) { return a + ((int64_t(b) * nf + f) * NK + (k + 1)) * P + pc; };
+  if (cell) {
+    *out(B.rho, 0, 1) = S[HF_R * P + pc];
+    for (int d = 0; d < 3; ++d) *out(B.velocity, d, 3) = S[(HF_V + d) * P + pc];
+    const double Tn = S[HF_T * P + pc];
+    if (B.temp_source)
+      B.temp_source[((int64_t(b) * na + (k - 1)) * nt + (cj - 1)) * nl + (ci - 1)] = Tn - O[HF_T * L.C + tid];
+    *out(B.temperature, 0, 1) = Tn;
+    bool neg = false;
+    for (int s = 0; s < NS; ++s) {
+      *out(B.vert_vel, s, NS) = S[(HF_W + s) * P + pc];
+      const double nd = S[(HF_N + s) * P + pc];
+      neg = neg || nd < 0.0;
+      *out(B.ndensity_s, s, GITM_NSPECIES_TOTAL) = nd;
+    }
+    if (neg) atomicOr(&A.status[b], GITM_ST_NEG_DENSITY);  // the reference stops (:359-372)
+    if (prm.use_ion_advection) {
+      const bool div = prm.use_improved_ion_advection != 0;
+      double change = 0.0;
+      if (div) {
+        // DivIVelocityLocal at the cell (:423-509): UAM_Gradient's component
+        // iDir of IVelocityPar(iDir) plus the latitude and radial terms
+        const double* VI = prm.non_magnetic ? B.ivelocity : B.ivelocity_par;
+        auto vi = [&](int d, int i, int j, int kk) {
+          return VI[((int64_t(b) * 3 + d) * NK + (kk + 1)) * P + int64_t(j + 1) * NI + (i + 1)];
+        };
+        const double InvR = GC[3 * L.C + tid];
+        double D = 0.0;
+        double g = 0.0;
+        if (nl > 1) {
+          const double InvCosLat = 1. / fmax(CosLat, 0.17);
+          const int64_t o = int64_t(b) * nl + (ci - 1);
+          g = (B.grad_lon_m[o] * vi(0, ci - 1, cj, k) + B.grad_lon_0[o] * vi(0, ci, cj, k) +
+               B.grad_lon_p[o] * vi(0, ci + 1, cj, k)) * InvR * InvCosLat;
+        }
+        D = D + g;
+        g = 0.0;
+        if (nt > 1) {
+          const int64_t o = int64_t(b) * nt + (cj - 1);
+          g = (B.grad_lat_m[o] * vi(1, ci, cj - 1, k) + B.grad_lat_0[o] * vi(1, ci, cj, k) +
+               B.grad_lat_p[o] * vi(1, ci, cj + 1, k)) * InvR;
+        }
+        D = D + g;
+        double tl = TanLat;
+        if (tl > 5.0) tl = 5.0;
+        if (tl < -5.0) tl = -5.0;
+        D = D - tl * vi(1, ci, cj, k) * InvR;
+        g = 0.0;
+        if (na > 1) {
+          const double* Rg = B.radial_distance + int64_t(b) * V + int64_t(cj + 1) * NI + (ci + 1);
+          const double Drp = Rg[(k + 2) * P] - Rg[(k + 1) * P];
+          const double Drm = Rg[(k + 1) * P] - Rg[k * P];
+          const double DrmOverDrp = Drm / Drp;
+          const double Drr2 = DrmOverDrp * DrmOverDrp;
+          const double Bottom = Drm * (1 + DrmOverDrp);
+          g = (Drr2 * vi(2, ci, cj, k + 1) - vi(2, ci, cj, k - 1) - (Drr2 - 1) * vi(2, ci, cj, k)) / Bottom;
+        }
+        D = D + g;
+        D = D + 2 * vi(2, ci, cj, k) * InvR;
+        D = D * CosLat;
+        change = dt * D;
+      }
+      double e = 0.0;
+      for (int s = 0; s < NI_ALL; ++s) {
+        double v;
+        if (s < NADV) {
+          v = S[(HF_I + s) * P + pc];
+          if (v < 1.0e2) v = 1.0e2;  // :400-412
+          if (div) v = v / (1 + change);
+          *out(B.idensity_s, s, GITM_NIONS) = v;
+        } else {
+          v = *out(B.idensity_s, s, GITM_NIONS);
+        }
+        e = e + v;
+      }
+      *out(B.idensity_s, GITM_NIONS - 1, GITM_NIONS) = e;
+    }
+  }
+  // with the divergence term the reference sums the electrons on every cell
+  // (:512-515): this plane's ghost ring, and the ghost planes of the block
+  if (prm.use_ion_advection && prm.use_improved_ion_advection) {
+    auto esum = [&](int64_t off) {  // off: index of a cell in field 0's block array
+      double e = 0.0;
+      for (int s = 0; s < NI_ALL; ++s) e = e + B.idensity_s[off + int64_t(s) * V];
+      B.idensity_s[off + int64_t(GITM_NIONS - 1) * V] = e;
+    };
+    const int64_t base = int64_t(b) * GITM_NIONS * V;
+    for (int c = tid; c < P; c += NT) {
+      const int i = c % NI - 1, j = c / NI - 1;
+      if (i >= 1 && i <= nl && j >= 1 && j <= nt) continue;
+      esum(base + (k + 1) * P + c);
+    }
+    if (k == 1)
+      for (int64_t c = tid; c < 2 * P; c += NT) esum(base + c);  // altitudes -1, 0
+    if (k == na)
+      for (int64_t c = tid; c < 2 * P; c += NT) esum(base + (na + 2) * P + c);  // nAlts+1, nAlts+2
+  }
+}
+
+}  // namespace
+
+size_t hz_smem_bytes(int n_lons, int n_lats) { return size_t(hz_layout(n_lons, n_lats).stride) * sizeof(double); }
+
+int hz_threads(int n_lons, int n_lats) {
+  const int c = n_lons * n_lats;
+  return c <= 128 ? 128 : (c <= 256 ? 256 : 0);
+}
+
+cudaError_t hz_launch(const GitmHzParams& prm, const GitmHzBlocks& b, double dt, uint32_t* status,
+                      cudaStream_t stream) {
+  HzArgs a;
+  a.prm = prm;
+  a.b = b;
+  a.dt = dt;
+  a.status = status;
+  const int nt = hz_threads(b.n_lons, b.n_lats);
+  const size_t smem = hz_smem_bytes(b.n_lons, b.n_lats);
+  const void* fn = (nt == 128) ? (const void*)hz_step_kernel<128> : (const void*)hz_step_kernel<256>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  void* args[] = {&a};
+  return cudaLaunchKernel(fn, dim3(unsigned(int64_t(b.n_blocks) * b.n_alts)), dim3(nt), args, smem, stream);
+}
+
+}  // namespace gv

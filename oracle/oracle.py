@@ -30,6 +30,7 @@ def _stale(path: str) -> bool:
     t = os.path.getmtime(path)
     srcs = [os.path.join(_HERE, f) for f in os.listdir(_HERE) if f.endswith((".cpp", ".hpp"))]
     srcs.append(os.path.join(_HERE, "..", "include", "gitm_vert.h"))
+    srcs.append(os.path.join(_HERE, "..", "include", "gitm_hz.h"))
     return any(os.path.getmtime(s) > t for s in srcs if os.path.exists(s))
 
 
@@ -63,6 +64,9 @@ def lib():
         L.oracle_mesh_coefs.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oracle_abi_sizes.restype = None
         L.oracle_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
+        L.oracle_hz_advance.restype = C.c_uint32
+        L.oracle_hz_advance.argtypes = [C.POINTER(abi.GitmHzParams), C.POINTER(abi.GitmHzBlocks), C.c_double,
+                                        C.POINTER(C.c_uint32), C.c_int]
         _LIB = L
     return _LIB
 
@@ -152,7 +156,17 @@ def mesh_coefs(alt: np.ndarray):
     return out[: 5 * n].reshape(n, 5), out[5 * n: 5 * n + 10].reshape(2, 5), out[5 * n + 10:].reshape(2, 5)
 
 
+def hz_advance(blocks, params, dt: float, nthreads: int | None = None):
+    """advance_horizontal for every block of host HzBlocks, in place; returns
+    the per-block status words."""
+    b = blocks.batch()
+    st = np.zeros(blocks.n_blocks, dtype=np.uint32)
+    nthreads = nthreads or os.cpu_count() or 1
+    lib().oracle_hz_advance(C.byref(params), C.byref(b), dt, st.ctypes.data_as(C.POINTER(C.c_uint32)), nthreads)
+    return st
+
+
 def abi_sizes():
-    out = (C.c_int64 * 7)()
+    out = (C.c_int64 * 9)()
     lib().oracle_abi_sizes(out)
     return list(out)

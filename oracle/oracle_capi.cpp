@@ -16,6 +16,7 @@
 
 #include "gitm_vert_oracle.hpp"
 #include "oracle_ausm.hpp"
+#include "oracle_hz.hpp"
 #include "flop_counter.hpp"
 
 using namespace gvo;
@@ -294,6 +295,20 @@ uint32_t oracle_advance_1d(const GitmVertParams* prm, const GitmModVerticalBatch
   return acc.load();
 }
 
+// advance_horizontal (advance_horizontal.f90:58-924) for every block; blocks
+// are independent and split over host threads.  status: one word per block
+// (may be NULL).  Returns the OR of all words.
+uint32_t oracle_hz_advance(const GitmHzParams* prm, const GitmHzBlocks* b, double dt, uint32_t* status,
+                           int nthreads) {
+  std::atomic<uint32_t> acc{0};
+  parallel_for(b->n_blocks, nthreads, [&](int64_t k) {
+    const uint32_t st = gvo_hz::advance_horizontal_block(*prm, *b, int(k), dt);
+    if (status) status[k] = st;
+    acc.fetch_or(st);
+  });
+  return acc.load();
+}
+
 // calc_timestep_vertical (calc_timestep.f90:85-157) for one member: cMax for
 // cells 0..nAlts+1 is written to cmax (native layout) and the local CFL time
 // step min over columns is returned (the caller takes the min with Dt and
@@ -414,7 +429,7 @@ void oracle_mesh_coefs(int nAlts, const double* alt, double* out) {
 }
 
 // sizeof of the ABI structs as the C compiler lays them out.
-void oracle_abi_sizes(int64_t out[7]) {
+void oracle_abi_sizes(int64_t out[9]) {
   out[0] = sizeof(GitmVertParams);
   out[1] = sizeof(GitmColumnBatch);
   out[2] = sizeof(GitmModVerticalBatch);
@@ -422,6 +437,8 @@ void oracle_abi_sizes(int64_t out[7]) {
   out[4] = sizeof(GitmFArray);
   out[5] = sizeof(GitmFortranState);
   out[6] = sizeof(GitmColumnAdjoint);
+  out[7] = sizeof(GitmHzParams);
+  out[8] = sizeof(GitmHzBlocks);
 }
 
 }  // extern "C"

@@ -12,9 +12,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    src = open(os.path.join(ROOT, "include", "gitm_vert.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(gitm_vert_\w+)\s*\(", src)))
+    """Every gitm_* function declared in include/*.h."""
+    names = set()
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names.update(re.findall(r"\b(gitm_(?:vert|hz)_\w+)\s*\(", src))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
@@ -26,7 +32,8 @@ def libpath():
 def test_header_declares_entry_points():
     syms = declared_symbols()
     for s in ("gitm_vert_create", "gitm_vert_plan_advance", "gitm_vert_advance_fortran",
-              "gitm_vert_advance_1d", "gitm_vert_cfl_dt", "gitm_vert_advance_native_host"):
+              "gitm_vert_advance_1d", "gitm_vert_cfl_dt", "gitm_vert_advance_native_host",
+              "gitm_hz_advance", "gitm_hz_status"):
         assert s in syms
 
 
@@ -45,7 +52,7 @@ def test_struct_sizes_match_header(oracle_lib):
     sizes = oracle_lib.abi_sizes()
     py = [C.sizeof(t) for t in (abi.GitmVertParams, abi.GitmColumnBatch, abi.GitmModVerticalBatch,
                                 abi.GitmLaunchConfig, abi.GitmFArray, abi.GitmFortranState,
-                                abi.GitmColumnAdjoint)]
+                                abi.GitmColumnAdjoint, abi.GitmHzParams, abi.GitmHzBlocks)]
     assert sizes == py
 
 
