@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--ens-members", type=int, default=48)
     ap.add_argument("--ens-steps", type=int, default=200)
     ap.add_argument("--ens-plain-steps", type=int, default=3)
+    ap.add_argument("--horizontal", action="store_true",
+                    help="measure the horizontal advance (advance_horizontal) on a globe of 9x9 blocks")
+    ap.add_argument("--hz-deg", type=float, default=1.0)
+    ap.add_argument("--hz-steps", type=int, default=50)
     return ap.parse_args()
 
 
@@ -695,8 +699,126 @@ def run_ensemble(args):
         print(json.dumps(out))
 
 
+def measured_hbm_peak() -> float:
+    """The measured HBM copy bandwidth (GB/s) of this pool's B200s, else the
+    earlier pool measurement of 6.65 TB/s."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def hz_bytes_per_block(n_lons: int, n_lats: int, n_alts: int) -> int:
+    """Compulsory DRAM bytes of one block per advance_horizontal: every block
+    array the step reads, once (the state's 28 fields: Rho, Temperature,
+    Velocity, VerticalVelocity, the six NDensityS, IDensityS; Gamma, two
+    cMax and two IVelocity components, IVelocityPar, RadialDistance and its
+    inverse, the six lon / lat distances) with its ghost cells, and the
+    interior cells it writes (22 fields and HorizontalTempSource)."""
+    whole = (n_lons + 4) * (n_lats + 4) * (n_alts + 4)
+    interior = n_lons * n_lats * n_alts
+    read = (2 + 3 + 6 + 6 + 10) + (1 + 2 + 2 + 3 + 2 + 6)
+    written = 2 + 3 + 6 + 6 + 3 + 1
+    return 8 * (read * whole + written * interior)
+
+
+def run_horizontal(args):
+    """advance_horizontal (gitm_hz_advance) on a globe of 9 x 9 blocks at
+    hz_deg: one launch per step over every (block, altitude) plane, state
+    resident in HBM; cell-steps/s = interior cells x steps / device time.
+    CPU baseline: the oracle on the host cores on a sample of the blocks."""
+    import torch
+
+    from gitm_b200 import abi
+    from gitm_b200 import horizontal as H
+    from gitm_b200 import vertical as V
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    nl = nt = 9
+    nbl = int(round(360.0 / args.hz_deg)) // nl
+    nbt = int(round(180.0 / args.hz_deg)) // nt
+    blocks = H.synthetic_blocks(nl, nt, args.n_alts, nbl, nbt, seed=rank)
+    cells = nl * nt * args.n_alts * blocks.n_blocks
+    p = abi.default_hz_params()
+    ctx = V.VerticalContext(abi.default_params(), device=local)
+    d = blocks.to_device(torch.device("cuda", local))
+    # the synthetic globe has no polar filter: at 1 deg the cells next to the
+    # poles are ~1 km wide in longitude and a 2 s step exceeds their CFL
+    # limit, so the state goes back to the initial one every `chunk` steps
+    # (outside the timed region)
+    snap = {k: d.arrays[k].clone() for k in H.OUTPUTS}
+
+    def restore():
+        for k in H.OUTPUTS:
+            d.arrays[k].copy_(snap[k])
+    chunk = 4
+    for _ in range(max(args.warmup, 3)):
+        H.advance_horizontal(ctx, d, DT, p)
+    restore()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    stream = torch.cuda.current_stream()
+    from gitm_b200._lib import lib
+    import ctypes as C
+    b = d.batch()
+    el = 0.0
+    n_chunks = max(1, -(-args.hz_steps // chunk))
+    for _ in range(n_chunks):
+        restore()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(chunk):
+            rc = lib().gitm_hz_advance(ctx.handle, C.byref(p), C.byref(b), DT, C.c_void_p(stream.cuda_stream))
+            if rc:
+                raise RuntimeError(ctx.last_error())
+        e1.record(stream)
+        e1.synchronize()
+        el += e0.elapsed_time(e1) / 1e3
+    args.hz_steps = n_chunks * chunk
+    clk = clocks.stop()
+    word, nbad = H.hz_status(ctx, clear=True)
+    ctx.close()
+    cb = None
+    if rank == 0 and args.cpu_seconds > 0:
+        from oracle import oracle
+        threads = os.cpu_count() or 1
+        nsample = min(blocks.n_blocks, max(threads, 64))
+        sample = H.HzBlocks(nl, nt, args.n_alts, nsample,
+                            {k: np.ascontiguousarray(v[:nsample]) for k, v in blocks.arrays.items()})
+        t0 = time.perf_counter()
+        oracle.hz_advance(sample, p, DT, nthreads=threads)
+        ec = time.perf_counter() - t0
+        cb = {"value": nl * nt * args.n_alts * nsample / ec, "unit": "cell-steps/s", "cores": threads,
+              "kind": "port", "sample": f"{nsample} of {blocks.n_blocks} blocks x 1 step, C++ oracle -O3, "
+                                        f"{threads} threads, {ec:.1f} s"}
+    if rank == 0:
+        per_step = el / args.hz_steps
+        bytes_step = hz_bytes_per_block(nl, nt, args.n_alts) * blocks.n_blocks
+        peak = measured_hbm_peak()
+        out = {"metric": f"cell-steps/s, horizontal advance, {args.hz_deg:g} deg globe of 9x9 blocks",
+               "value": cells / per_step, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.hz_steps,
+               "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * per_step, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+               "config": {"workload": f"{blocks.n_blocks} blocks of {nl}x{nt} cells, {args.n_alts} alts, "
+                                      f"advance_horizontal RK4, dt 2 s, improved ion advection",
+                          "l2": "state larger than L2 (no flush needed)", "launch": "one CTA per (block, altitude) "
+                          "plane, one launch per step", "state_restored_every": 4},
+               "clocks": clk, "gpu_launches": args.hz_steps, "status": {"or": word, "bad_blocks": nbad},
+               "roofline_hbm": {"bound": "hbm", "achieved": bytes_step / per_step / 1e9, "peak": peak,
+                                "unit": "GB/s", "frac": bytes_step / per_step / 1e9 / peak,
+                                "bytes_per_step": bytes_step,
+                                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+               "cpu_baseline": cb}
+        print(json.dumps(out))
+
+
 def main():
     args = parse()
+    if args.horizontal:
+        run_horizontal(args)
+        return
     if args.ensemble:
         run_ensemble(args)
         return

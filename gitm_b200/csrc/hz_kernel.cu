@@ -40,7 +40,7 @@ constexpr double F2 = 0.0416667;  // Factor2, advance_horizontal.f90:940
 // Shared-memory plan of one plane: P cells with ghosts, C interior cells.
 struct HzLayout {
   int P, C;
-  int S, O, K, G, GC, stride;
+  int S, K, G, GC, stride;
 };
 
 __host__ __device__ inline HzLayout hz_layout(int nLons, int nLats) {
@@ -49,7 +49,6 @@ __host__ __device__ inline HzLayout hz_layout(int nLons, int nLats) {
   L.C = nLons * nLats;
   int o = 0;
   L.S = o;  o += HZ_NSW * L.P;
-  L.O = o;  o += HZ_NSW * L.C;
   L.K = o;  o += HZ_NSW * L.C;  // the stage's New - state of every field
   L.G = o;  o += HZ_NGP * L.P;
   L.GC = o; o += HZ_NGC * L.C;
@@ -117,8 +116,8 @@ struct HzArgs {
   uint32_t* status;  // one word per block
 };
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1) hz_step_kernel(const HzArgs A) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) hz_step_kernel(const HzArgs A) {
   extern __shared__ double sm[];
   const GitmHzBlocks& B = A.b;
   const GitmHzParams& prm = A.prm;
@@ -138,7 +137,6 @@ __global__ void __launch_bounds__(NT, 1) hz_step_kernel(const HzArgs A) {
 
   // ---------------------------------------------------------------- load
   double* S = sm + L.S;
-  double* O = sm + L.O;
   double* Kc = sm + L.K;
   double* GP = sm + L.G;
   double* GC = sm + L.GC;
@@ -173,9 +171,8 @@ __global__ void __launch_bounds__(NT, 1) hz_step_kernel(const HzArgs A) {
     GC[5 * L.C + tid] = plane(B.ivelocity, 0, 3)[pc];
     GC[6 * L.C + tid] = plane(B.ivelocity, 1, 3)[pc];
   }
-  __syncthreads();
-  if (cell)
-    for (int f = 0; f < HZ_NSW; ++f) O[f * L.C + tid] = S[f * P + pc];
+  // Orig (:181-186) stays in the input arrays: they are written only by the
+  // store phase, after the last stage
 
   // per-cell constants of the equations (:680-686)
   double SinLat = 0.0, CosLat = 0.0, TanLat = 0.0;
@@ -274,7 +271,7 @@ __global__ void __launch_bounds__(NT, 1) hz_step_kernel(const HzArgs A) {
     if (cell) {
 #pragma unroll
       for (int f = 0; f < HZ_NSW; ++f) {
-        const double o = O[f * L.C + tid];
+        const double o = src_of(f)[pc];
         const double kf = Kc[f * L.C + tid];
         double nx;
         if (st == 0) {
@@ -303,7 +300,7 @@ __global__ void __launch_bounds__(NT, 1) hz_step_kernel(const HzArgs A) {
     for (int d = 0; d < 3; ++d) *out(B.velocity, d, 3) = S[(HF_V + d) * P + pc];
     const double Tn = S[HF_T * P + pc];
     if (B.temp_source)
-      B.temp_source[((int64_t(b) * na + (k - 1)) * nt + (cj - 1)) * nl + (ci - 1)] = Tn - O[HF_T * L.C + tid];
+      B.temp_source[((int64_t(b) * na + (k - 1)) * nt + (cj - 1)) * nl + (ci - 1)] = Tn - src_of(HF_T)[pc];
     *out(B.temperature, 0, 1) = Tn;
     bool neg = false;
     for (int s = 0; s < NS; ++s) {
@@ -402,7 +399,7 @@ size_t hz_smem_bytes(int n_lons, int n_lats) { return size_t(hz_layout(n_lons, n
 
 int hz_threads(int n_lons, int n_lats) {
   const int c = n_lons * n_lats;
-  return c <= 128 ? 128 : (c <= 256 ? 256 : 0);
+  return c <= 96 ? 96 : (c <= 128 ? 128 : (c <= 256 ? 256 : 0));
 }
 
 cudaError_t hz_launch(const GitmHzParams& prm, const GitmHzBlocks& b, double dt, uint32_t* status,
@@ -414,7 +411,9 @@ cudaError_t hz_launch(const GitmHzParams& prm, const GitmHzBlocks& b, double dt,
   a.status = status;
   const int nt = hz_threads(b.n_lons, b.n_lats);
   const size_t smem = hz_smem_bytes(b.n_lons, b.n_lats);
-  const void* fn = (nt == 128) ? (const void*)hz_step_kernel<128> : (const void*)hz_step_kernel<256>;
+  // 96 threads: 9 x 9 blocks (GITM's usual size) at 4 CTAs per SM
+  const void* fn = (nt == 96) ? (const void*)hz_step_kernel<96, 4>
+                 : (nt == 128) ? (const void*)hz_step_kernel<128, 3> : (const void*)hz_step_kernel<256, 1>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
