@@ -709,17 +709,19 @@ def measured_hbm_peak() -> float:
 
 
 def hz_bytes_per_block(n_lons: int, n_lats: int, n_alts: int) -> int:
-    """Compulsory DRAM bytes of one block per advance_horizontal: every block
-    array the step reads, once (the state's 28 fields: Rho, Temperature,
-    Velocity, VerticalVelocity, the six NDensityS, IDensityS; Gamma, two
-    cMax and two IVelocity components, IVelocityPar, RadialDistance and its
-    inverse, the six lon / lat distances) with its ghost cells, and the
-    interior cells it writes (22 fields and HorizontalTempSource)."""
+    """DRAM bytes of one block per advance_horizontal, counted from above:
+    every block array the step reads, once, whole (the state's 27 fields:
+    Rho, Temperature, Velocity, VerticalVelocity, the six NDensityS,
+    IDensityS; Gamma, two IVelocity components, IVelocityPar,
+    RadialDistance and its inverse, the six lon / lat distances; two
+    components of cMax_GDB with its one ghost cell), and the interior cells
+    it writes (21 fields and HorizontalTempSource)."""
     whole = (n_lons + 4) * (n_lats + 4) * (n_alts + 4)
+    cmax = (n_lons + 2) * (n_lats + 2) * (n_alts + 2)
     interior = n_lons * n_lats * n_alts
-    read = (2 + 3 + 6 + 6 + 10) + (1 + 2 + 2 + 3 + 2 + 6)
+    read = (2 + 3 + 6 + 6 + 10) + (1 + 2 + 3 + 2 + 6)
     written = 2 + 3 + 6 + 6 + 3 + 1
-    return 8 * (read * whole + written * interior)
+    return 8 * (read * whole + 2 * cmax + written * interior)
 
 
 def run_horizontal(args):

@@ -153,11 +153,22 @@ __global__ void __launch_bounds__(NT, MINB) hz_step_kernel(const HzArgs A) {
     for (int c = tid; c < P; c += NT) S[f * P + c] = src[c];
   }
   {
-    const double* gsrc[HZ_NGP] = {plane(B.inv_dlon_dist_fb, 0, 1), plane(B.dlon_dist_fb, 0, 1),
-                                  plane(B.inv_dlat_dist_fb, 0, 1), plane(B.dlat_dist_fb, 0, 1),
-                                  plane(B.cmax, 0, 3), plane(B.cmax, 1, 3)};
-    for (int g = 0; g < HZ_NGP; ++g)
+    const double* gsrc[4] = {plane(B.inv_dlon_dist_fb, 0, 1), plane(B.dlon_dist_fb, 0, 1),
+                             plane(B.inv_dlat_dist_fb, 0, 1), plane(B.dlat_dist_fb, 0, 1)};
+    for (int g = 0; g < 4; ++g)
       for (int c = tid; c < P; c += NT) GP[g * P + c] = gsrc[g][c];
+    // cMax_GDB(0:nLons+1, 0:nLats+1, 0:nAlts+1, 3, nBlocks): east and north
+    // components of this altitude into planes with the outer ghost ring
+    // (never read) zeroed
+    const int ci2 = nl + 2, cj2 = nt + 2;
+    for (int d = 0; d < 2; ++d) {
+      const double* cm = B.cmax + (((int64_t(b) * 3 + d) * (na + 2) + k) * cj2) * ci2;
+      for (int c = tid; c < P; c += NT) {
+        const int i = c % NI - 1, j = c / NI - 1;  // Fortran indices
+        const bool in = (i >= 0 && i <= nl + 1 && j >= 0 && j <= nt + 1);
+        GP[(4 + d) * P + c] = in ? cm[j * ci2 + i] : 0.0;
+      }
+    }
   }
   const bool cell = tid < L.C;
   const int ci = cell ? tid % nl + 1 : 1, cj = cell ? tid / nl + 1 : 1;  // Fortran (iLon, iLat)

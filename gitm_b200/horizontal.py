@@ -178,13 +178,14 @@ def synthetic_blocks(n_lons: int = 9, n_lats: int = 9, n_alts: int = 50, n_block
     ivp[:, 1] = mod(30.0)
     ivp[:, 2] = mod(40.0)
     A["ivelocity_par"] = ivp
-    # cMax_GDB east / north as calc_timestep_horizontal forms them: |V| + sound speed
+    # cMax_GDB(0:nLons+1, 0:nLats+1, 0:nAlts+1, 3, nBlocks) as
+    # calc_timestep_horizontal forms its east / north parts: |V| + sound speed
     cs = np.sqrt(A["gamma"] * A["temperature"])
     cm = np.zeros((nb, 3, NK, NJ, NI))
     cm[:, 0] = np.abs(vel[:, 0]) + cs
     cm[:, 1] = np.abs(vel[:, 1]) + cs
     cm[:, 2] = np.abs(vel[:, 2]) + cs
-    A["cmax"] = cm
+    A["cmax"] = np.ascontiguousarray(cm[:, :, 1:-1, 1:-1, 1:-1])
     # geometry (initialize.f90:193-291)
     RR = np.broadcast_to(R[None, :, None, None], shape)
     A["radial_distance"] = np.ascontiguousarray(RR)

@@ -63,7 +63,8 @@ typedef struct GitmHzBlocks {
                              NewTemp - Temperature; may be NULL          */
   /* read */
   const double* gamma;    /* Gamma                block array            */
-  const double* cmax;     /* cMax_GDB             block array [3]        */
+  const double* cmax;     /* cMax_GDB(0:nLons+1, 0:nLats+1, 0:nAlts+1, 3, nBlocks)
+                             (ModGITM.f90:250: one ghost cell, not two) */
   const double* ivelocity;      /* IVelocity      block array [3]        */
   const double* ivelocity_par;  /* IVelocityPar   block array [3] (NULL when
                                    non_magnetic or without the divergence) */

@@ -99,6 +99,10 @@ inline uint32_t advance_horizontal_block(const GitmHzParams& prm, const GitmHzBl
   auto blkf = [&](const double* a, int i, int j, int k, int f, int nf) { return a[S.at(i, j, k, f, nf, b)]; };
   auto lat1 = [&](const double* a, int j) { return a[int64_t(b) * (nLats + 4) + (j + 1)]; };
   auto B_set = [](double* a, int64_t o, double v) { a[o] = v; };
+  // cMax_GDB(0:nLons+1, 0:nLats+1, 0:nAlts+1, 3, nBlocks)
+  auto cmax = [&](int i, int j, int k, int d) {
+    return B.cmax[((((int64_t(b) * 3 + d) * (nAlts + 2) + k) * (nLats + 2) + j) * (nLons + 2)) + i];
+  };
 
   // the 2-D planes of the current altitude (:87-95)
   Plane Rho_C, Temp_C, gamma_C;
@@ -154,7 +158,7 @@ inline uint32_t advance_horizontal_block(const GitmHzParams& prm, const GitmHzBl
               [&](int i) { return blk(B.dlon_dist_fb, i, iLat, iAlt); }, prm.beta_limiter, VarWest, VarEast);
           std::vector<double> DiffFlux(nLons + 2);
           for (int i = 1; i <= nLons + 1; ++i)
-            DiffFlux[i] = 0.5 * std::max(blkf(B.cmax, i - 1, iLat, iAlt, iEast, 3), blkf(B.cmax, i, iLat, iAlt, iEast, 3)) *
+            DiffFlux[i] = 0.5 * std::max(cmax(i - 1, iLat, iAlt, iEast), cmax(i, iLat, iAlt, iEast)) *
                           (VarEast[i] - VarWest[i]);
           for (int i = 1; i <= nLons; ++i) {
             const double InvdLon = blk(B.inv_dlon_dist_gb, i, iLat, iAlt);
@@ -173,7 +177,7 @@ inline uint32_t advance_horizontal_block(const GitmHzParams& prm, const GitmHzBl
           std::vector<double> DiffFlux(nLats + 2);
           for (int j = 1; j <= nLats + 1; ++j)
             DiffFlux[j] = 0.5 *
-                          std::max(blkf(B.cmax, iLon, j - 1, iAlt, iNorth, 3), blkf(B.cmax, iLon, j, iAlt, iNorth, 3)) *
+                          std::max(cmax(iLon, j - 1, iAlt, iNorth), cmax(iLon, j, iAlt, iNorth)) *
                           (VarNorth[j] - VarSouth[j]);
           for (int j = 1; j <= nLats; ++j) {
             const double InvdLat = blk(B.inv_dlat_dist_gb, iLon, j, iAlt);

@@ -14,8 +14,9 @@ def _uniform(blocks):
     A = blocks.arrays
     for name in ("rho", "temperature", "gamma"):
         A[name][:] = A[name][:, :, 2:3, 2:3]
-    for name in ("velocity", "vert_vel", "ndensity_s", "idensity_s", "ivelocity", "cmax"):
+    for name in ("velocity", "vert_vel", "ndensity_s", "idensity_s", "ivelocity"):
         A[name][:] = A[name][:, :, :, 2:3, 2:3]
+    A["cmax"][:] = A["cmax"][:, :, :, 1:2, 1:2]
     A["velocity"][:, 0:2] = 0.0
     return blocks
 
