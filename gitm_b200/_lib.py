@@ -49,6 +49,7 @@ SIGNATURES = {
     # include/gitm_hz.h
     "gitm_hz_advance": (C.c_int, [_P, C.POINTER(abi.GitmHzParams), C.POINTER(abi.GitmHzBlocks), C.c_double, _P]),
     "gitm_hz_status": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_int]),
+    "gitm_hz_exchange": (C.c_int, [_P, C.POINTER(abi.GitmHzExchange), _P]),
 }
 
 

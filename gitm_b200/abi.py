@@ -27,6 +27,7 @@ ST_LU_SINGULAR = 4
 ST_NONFINITE = 8
 ST_BAD_NALTS = 16
 ST_ADJ_BRANCH = 32
+ST_LOW_TEMPERATURE = 64  # the horizontal exchange's Temperature < 100 check
 
 SOLVER_RUSANOV = 0
 SOLVER_AUSM = 1
@@ -243,6 +244,17 @@ def default_hz_params(**overrides) -> GitmHzParams:
 class GitmHzBlocks(C.Structure):
     _fields_ = [("n_lons", C.c_int32), ("n_lats", C.c_int32), ("n_alts", C.c_int32), ("n_blocks", C.c_int32)] + \
         [(name, _dp) for name in HZ_BLOCK_FIELDS]
+
+
+HZ_EXCHANGE_FIELDS = ("rho", "temperature", "itemperature", "etemperature", "velocity", "vert_vel", "ndensity_s",
+                      "idensity_s", "ivelocity", "ivelocity_par", "latitude")
+
+
+class GitmHzExchange(C.Structure):
+    _fields_ = [("n_lons", C.c_int32), ("n_lats", C.c_int32), ("n_alts", C.c_int32), ("n_blocks_lon", C.c_int32),
+                ("n_blocks_lat", C.c_int32), ("north_pole", C.c_int32), ("south_pole", C.c_int32),
+                ("use_ion_advection", C.c_int32), ("non_magnetic", C.c_int32), ("reserved0", C.c_int32)] + \
+        [(name, _dp) for name in HZ_EXCHANGE_FIELDS]
 
 
 def dptr(addr: int):

@@ -1732,6 +1732,42 @@ extern "C" int gitm_hz_advance(GitmVertCtx* ctx, const GitmHzParams* params, con
   return GITM_OK;
 }
 
+extern "C" int gitm_hz_exchange(GitmVertCtx* ctx, const GitmHzExchange* x, void* stream) {
+  if (!ctx || !x) return set_err(ctx, GITM_ERR_ARG, "bad arguments");
+  if (x->n_lons < 2 || x->n_lats < 2 || x->n_alts < 1 || x->n_blocks_lon < 1 || x->n_blocks_lat < 1)
+    return set_err(ctx, GITM_ERR_ARG, "bad block grid (the two-cell ghost ring needs blocks of 2 x 2 cells or more)");
+  if ((x->north_pole || x->south_pole) && (x->n_blocks_lon % 2 != 0))
+    return set_err(ctx, GITM_ERR_UNSUPPORTED, "a pole connection needs an even number of blocks in longitude");
+  const int64_t nb = int64_t(x->n_blocks_lon) * x->n_blocks_lat;
+  if (nb * x->n_alts > int64_t(0x7fffffff)) return set_err(ctx, GITM_ERR_ARG, "too many (block, altitude) planes");
+  const void* req[] = {x->rho, x->temperature, x->velocity, x->vert_vel, x->ndensity_s, x->latitude,
+                       x->non_magnetic ? x->ivelocity : x->ivelocity_par};
+  for (const void* p : req)
+    if (!p || !is_device_ptr(p)) return set_err(ctx, GITM_ERR_ARG, "the exchanged arrays must be non-NULL device pointers");
+  if (x->use_ion_advection && (!x->idensity_s || !is_device_ptr(x->idensity_s)))
+    return set_err(ctx, GITM_ERR_ARG, "use_ion_advection needs IDensityS");
+  if (!is_device_ptr(x->itemperature) || !is_device_ptr(x->etemperature))
+    return set_err(ctx, GITM_ERR_ARG, "itemperature / etemperature must be device pointers or NULL");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (ctx->hz_status_n < nb) {
+    cudaFree(ctx->hz_status);
+    ctx->hz_status = nullptr;
+    ctx->hz_status_n = 0;
+    if (cudaMalloc(&ctx->hz_status, size_t(nb) * sizeof(uint32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, GITM_ERR_NOMEM, "cannot allocate the block status words");
+    }
+    ctx->hz_status_n = nb;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(ctx, cudaMemsetAsync(ctx->hz_status, 0, size_t(nb) * sizeof(uint32_t), st));
+  cudaError_t e = hz_exchange_launch(*x, ctx->hz_status, st);
+  if (e != cudaSuccess) return set_err(ctx, GITM_ERR_CUDA, "hz exchange launch: %s", cudaGetErrorString(e));
+  ctx->hz_blocks = nb;
+  ctx->hz_stream = st;
+  return GITM_OK;
+}
+
 extern "C" int gitm_hz_status(GitmVertCtx* ctx, uint32_t* or_out, int64_t* n_bad, int clear) {
   if (!ctx) return GITM_ERR_ARG;
   if (or_out) *or_out = 0;

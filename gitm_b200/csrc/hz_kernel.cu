@@ -404,7 +404,103 @@ __global__ void __launch_bounds__(NT, MINB) hz_step_kernel(const HzArgs A) {
   }
 }
 
+// exchange_messages_sphere (exchange_messages_sphere.f90:4-95) for one
+// (block, altitude) plane: the ghost ring takes the interior cells it
+// covers (longitude periodic; across a connected pole the cell mirrored in
+// latitude, n_blocks_lon / 2 blocks away -- the neighbours of
+// AB_SPH_module.f90:180-370 and the packing of AB_XFER_array_util.f90),
+// then the polar ghost rows' horizontal winds and ion velocities change sign
+// (:35-76, on every altitude: the CTAs of the first and last altitude also
+// take the ghost altitudes), then the checks of :78-88.
+__global__ void __launch_bounds__(128) hz_exchange_kernel(const GitmHzExchange X, uint32_t* status) {
+  const int nl = X.n_lons, nt = X.n_lats, na = X.n_alts;
+  const int NI = nl + 4, NJ = nt + 4, NK = na + 4;
+  const int64_t P = int64_t(NI) * NJ;
+  const int k = blockIdx.x % na + 1;
+  const int b = blockIdx.x / na;
+  const int bx = b % X.n_blocks_lon, by = b / X.n_blocks_lon;
+  const int64_t NLON = int64_t(nl) * X.n_blocks_lon, NLAT = int64_t(nt) * X.n_blocks_lat;
+  const int64_t half = int64_t(X.n_blocks_lon / 2) * nl;
+  double* VIw = X.non_magnetic ? X.ivelocity : X.ivelocity_par;
+  auto at = [&](double* a, int blk, int f, int nf, int kk, int64_t c) -> double& {
+    return a[((int64_t(blk) * nf + f) * NK + (kk + 1)) * P + c];
+  };
+  for (int c = threadIdx.x; c < P; c += blockDim.x) {
+    const int i = c % NI - 1, j = c / NI - 1;  // Fortran (iLon, iLat)
+    if (i >= 1 && i <= nl && j >= 1 && j <= nt) continue;
+    int64_t G = int64_t(bx) * nl + i, GJ = int64_t(by) * nt + j;  // global 1-based
+    if (GJ < 1) {
+      if (!X.south_pole) continue;
+      GJ = 1 - GJ;
+      G += half;
+    } else if (GJ > NLAT) {
+      if (!X.north_pole) continue;
+      GJ = 2 * NLAT + 1 - GJ;
+      G += half;
+    }
+    G = ((G - 1) % NLON + NLON) % NLON + 1;
+    const int sbx = int((G - 1) / nl), sby = int((GJ - 1) / nt);
+    const int si = int(G - int64_t(sbx) * nl), sj = int(GJ - int64_t(sby) * nt);
+    const int sb = sby * X.n_blocks_lon + sbx;
+    const int64_t sc = int64_t(sj + 1) * NI + (si + 1);
+    auto cp = [&](double* a, int f, int nf) { at(a, b, f, nf, k, c) = at(a, sb, f, nf, k, sc); };
+    cp(X.rho, 0, 1);
+    for (int d = 0; d < 3; ++d) cp(X.velocity, d, 3);
+    for (int s = 0; s < NS; ++s) cp(X.vert_vel, s, NS);
+    for (int s = 0; s < NS; ++s) cp(X.ndensity_s, s, GITM_NSPECIES_TOTAL);
+    cp(X.temperature, 0, 1);
+    if (X.itemperature) cp(X.itemperature, 0, 1);
+    if (X.etemperature) cp(X.etemperature, 0, 1);
+    if (X.use_ion_advection) {
+      for (int s = 0; s < GITM_NIONS; ++s) cp(X.idensity_s, s, GITM_NIONS);
+      for (int d = 0; d < 3; ++d) cp(VIw, d, 3);
+    }
+  }
+  __syncthreads();
+  // :35-76 -- Latitude(0) < -pi/2: rows -1:0; Latitude(nLats+1) > pi/2:
+  // rows nLats+1:nLats+2; every longitude, every altitude
+  const double lat0 = X.latitude[int64_t(b) * NJ + 1];
+  const double latn = X.latitude[int64_t(b) * NJ + nt + 2];
+  auto flip_plane = [&](int kk, int j0) {
+    for (int c = threadIdx.x; c < 2 * NI; c += blockDim.x) {
+      const int64_t cc = int64_t(j0 + 1 + c / NI) * NI + c % NI;
+      for (int d = 0; d < 2; ++d) {
+        at(X.velocity, b, d, 3, kk, cc) = -at(X.velocity, b, d, 3, kk, cc);
+        at(VIw, b, d, 3, kk, cc) = -at(VIw, b, d, 3, kk, cc);
+      }
+    }
+  };
+  const double PI_ = 3.141592653589793;
+  for (int side = 0; side < 2; ++side) {
+    const bool polar = side == 0 ? (lat0 < -PI_ / 2.0) : (latn > PI_ / 2.0);
+    if (!polar) continue;
+    const int j0 = side == 0 ? -1 : nt + 1;
+    flip_plane(k, j0);
+    if (k == 1) {
+      flip_plane(-1, j0);
+      flip_plane(0, j0);
+    }
+    if (k == na) {
+      flip_plane(na + 1, j0);
+      flip_plane(na + 2, j0);
+    }
+  }
+  // :78-88 on this altitude's interior
+  uint32_t w = 0;
+  for (int c = threadIdx.x; c < nl * nt; c += blockDim.x) {
+    const int64_t cc = int64_t(c / nl + 2) * NI + (c % nl + 2);
+    if (at(X.temperature, b, 0, 1, k, cc) < 100.0) w |= GITM_ST_LOW_TEMPERATURE;
+    if (at(X.rho, b, 0, 1, k, cc) < 0.0) w |= GITM_ST_NEG_DENSITY;
+  }
+  if (w) atomicOr(&status[b], w);
+}
+
 }  // namespace
+
+cudaError_t hz_exchange_launch(const GitmHzExchange& x, uint32_t* status, cudaStream_t stream) {
+  hz_exchange_kernel<<<unsigned(int64_t(x.n_blocks_lon) * x.n_blocks_lat * x.n_alts), 128, 0, stream>>>(x, status);
+  return cudaGetLastError();
+}
 
 size_t hz_smem_bytes(int n_lons, int n_lats) { return size_t(hz_layout(n_lons, n_lats).stride) * sizeof(double); }
 

@@ -18,5 +18,7 @@ int hz_threads(int n_lons, int n_lats);
 // One advance_horizontal for every block; status: one word per block.
 cudaError_t hz_launch(const GitmHzParams& prm, const GitmHzBlocks& b, double dt, uint32_t* status,
                       cudaStream_t stream);
+// exchange_messages_sphere over every (block, altitude) plane.
+cudaError_t hz_exchange_launch(const GitmHzExchange& x, uint32_t* status, cudaStream_t stream);
 
 }  // namespace gv

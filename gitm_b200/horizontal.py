@@ -42,10 +42,13 @@ class HzBlocks:
     n_alts: int
     n_blocks: int
     arrays: dict
+    n_blocks_lon: int = 0  # the sphere's block grid (block = iLat * n_blocks_lon + iLon), for the exchange
+    n_blocks_lat: int = 0
 
     def copy(self) -> "HzBlocks":
         return HzBlocks(self.n_lons, self.n_lats, self.n_alts, self.n_blocks,
-                        {k: (None if v is None else v.copy()) for k, v in self.arrays.items()})
+                        {k: (None if v is None else v.copy()) for k, v in self.arrays.items()},
+                        self.n_blocks_lon, self.n_blocks_lat)
 
     def batch(self) -> abi.GitmHzBlocks:
         """GitmHzBlocks of these arrays (host numpy or CUDA tensors)."""
@@ -69,7 +72,8 @@ class HzBlocks:
     def to_device(self, device="cuda") -> "HzBlocks":
         import torch
         return HzBlocks(self.n_lons, self.n_lats, self.n_alts, self.n_blocks,
-                        {k: (None if v is None else torch.from_numpy(v).to(device)) for k, v in self.arrays.items()})
+                        {k: (None if v is None else torch.from_numpy(v).to(device)) for k, v in self.arrays.items()},
+                        self.n_blocks_lon, self.n_blocks_lat)
 
     def to_numpy(self) -> dict:
         out = {}
@@ -96,6 +100,34 @@ def advance_horizontal(ctx, blocks: HzBlocks, dt: float, params=None, stream=Non
     word, nbad = hz_status(ctx, clear=True)
     if word:
         raise GitmStop(word, nbad, "advance_horizontal: negative neutral density")
+
+
+def exchange_batch(blocks: HzBlocks, north_pole=True, south_pole=True, use_ion_advection=True,
+                   non_magnetic=False) -> abi.GitmHzExchange:
+    """GitmHzExchange of these arrays (host numpy or CUDA tensors)."""
+    x = abi.GitmHzExchange()
+    x.n_lons, x.n_lats, x.n_alts = blocks.n_lons, blocks.n_lats, blocks.n_alts
+    x.n_blocks_lon, x.n_blocks_lat = blocks.n_blocks_lon, blocks.n_blocks_lat
+    x.north_pole, x.south_pole = int(north_pole), int(south_pole)
+    x.use_ion_advection, x.non_magnetic = int(use_ion_advection), int(non_magnetic)
+    for name in abi.HZ_EXCHANGE_FIELDS:
+        a = blocks.arrays.get(name)
+        addr = 0 if a is None else (a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+        setattr(x, name, abi.dptr(addr))
+    return x
+
+
+def exchange_messages(ctx, blocks: HzBlocks, stream=None, **flags):
+    """gitm_hz_exchange (exchange_messages_sphere) on device blocks; raises
+    GitmStop when a block's Temperature < 100 or Rho < 0 (the reference stops)."""
+    from ._lib import lib
+    from .vertical import GitmStop, _check
+    x = exchange_batch(blocks, **flags)
+    s = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
+    _check(lib().gitm_hz_exchange(ctx.handle, C.byref(x), C.c_void_p(s)), ctx.handle, "hz_exchange")
+    word, nbad = hz_status(ctx, clear=True)
+    if word:
+        raise GitmStop(word, nbad, "exchange_messages_sphere: Temperature < 100 or Rho < 0")
 
 
 def hz_status(ctx, clear: bool = False):
@@ -242,5 +274,8 @@ def synthetic_blocks(n_lons: int = 9, n_lats: int = 9, n_alts: int = 50, n_block
     A["grad_lon_m"], A["grad_lon_0"], A["grad_lon_p"] = grad_coefs(lon, n_lons)
     A["grad_lat_m"], A["grad_lat_0"], A["grad_lat_p"] = grad_coefs(lat, n_lats)
     A["temp_source"] = np.zeros((nb, n_alts, n_lats, n_lons))
+    # ion and electron temperatures (moved by the exchange, not read by the advance)
+    A["itemperature"] = np.ascontiguousarray(A["temperature"] * (1.1 + mod(0.02)))
+    A["etemperature"] = np.ascontiguousarray(A["temperature"] * (1.5 + mod(0.05)))
     A = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in A.items()}
-    return HzBlocks(n_lons, n_lats, n_alts, nb, A)
+    return HzBlocks(n_lons, n_lats, n_alts, nb, A, n_blocks_lon, n_blocks_lat)

@@ -39,6 +39,7 @@ STOP_MESSAGES = {
     abi.ST_BAD_NALTS: "nAlts outside the range of the launch",
     abi.ST_ADJ_BRANCH: "the adjoint met the upper ion boundary's negative-density repair, which it does "
                        "not differentiate",
+    abi.ST_LOW_TEMPERATURE: "Temperature < 100.0 (exchange_messages_sphere.f90:78-82)",
 }
 
 

@@ -35,6 +35,8 @@ extern "C" {
 #endif
 
 #define GITM_NSPECIES_TOTAL 11 /* nSpeciesTotal (ModEarth.f90:26): NDensityS's 4th extent */
+#define GITM_ST_LOW_TEMPERATURE 64u /* Temperature < 100 after the exchange
+                                       exchange_messages_sphere.f90:80-84 */
 
 typedef struct GitmHzParams {
   int32_t use_coriolis;               /* UseCoriolis                          */
@@ -95,7 +97,49 @@ typedef struct GitmHzBlocks {
 int gitm_hz_advance(GitmVertCtx* ctx, const GitmHzParams* params, const GitmHzBlocks* blocks, double dt,
                     void* stream);
 
-/* Status words of the last gitm_hz_advance, one per block: OR of all into
+/*
+ * The ghost cells of a whole sphere of blocks (exchange_messages_sphere,
+ * exchange_messages_sphere.f90:4-95, with the transfer of
+ * ModSphereInterface.f90:395-513 and srcSphereAB's multi-block packers,
+ * AB_XFER_array_util.f90, over the neighbours of AB_SPH_module.f90:
+ * 180-370).  Blocks tile the sphere as block = iLat * n_blocks_lon + iLon
+ * (0-based), south to north.  Every ghost cell of the two-cell ring at
+ * altitudes 1..nAlts takes the value of the interior cell it covers:
+ * longitude periodic, and across a connected pole the cell mirrored in
+ * latitude n_blocks_lon / 2 blocks away in longitude; then the east and
+ * north components of Velocity and of IVelocity / IVelocityPar are negated
+ * in the ghost rows beyond a pole (every longitude and altitude, as the
+ * reference does), and a block whose interior Temperature drops below 100
+ * or Rho below 0 gets GITM_ST_LOW_TEMPERATURE / GITM_ST_NEG_DENSITY
+ * (the reference stops).  n_blocks_lon must be even when a pole is
+ * connected (the corner neighbours across the pole pair up only then), and
+ * blocks hold 2 x 2 cells or more.
+ */
+typedef struct GitmHzExchange {
+  int32_t n_lons, n_lats, n_alts, n_blocks_lon, n_blocks_lat;
+  int32_t north_pole, south_pole;    /* connect across the poles (IsFullSphere: both) */
+  int32_t use_ion_advection;         /* UseIonAdvection: IDensityS and the ion velocity move too */
+  int32_t non_magnetic;              /* NonMagnetic: IVelocity instead of IVelocityPar */
+  int32_t reserved0;
+  double* rho;            /* Rho                      block array            */
+  double* temperature;    /* Temperature              block array            */
+  double* itemperature;   /* ITemperature             block array (may be NULL) */
+  double* etemperature;   /* eTemperature             block array (may be NULL) */
+  double* velocity;       /* Velocity                 block array [3]        */
+  double* vert_vel;       /* VerticalVelocity         block array [nSpecies] */
+  double* ndensity_s;     /* NDensityS                block array [nSpeciesTotal] */
+  double* idensity_s;     /* IDensityS                block array [nIons]    */
+  double* ivelocity;      /* IVelocity                block array [3]        */
+  double* ivelocity_par;  /* IVelocityPar             block array [3]        */
+  const double* latitude; /* Latitude(-1:nLats+2, nBlocks)                   */
+} GitmHzExchange;
+
+/* exchange_messages_sphere on device arrays, on `stream`; the status words
+ * (one per block) are read with gitm_hz_status.  Replaces
+ * exchange_messages_sphere.f90:4-95 for a single-process sphere. */
+int gitm_hz_exchange(GitmVertCtx* ctx, const GitmHzExchange* x, void* stream);
+
+/* Status words of the last gitm_hz_advance or gitm_hz_exchange, one per block: OR of all into
  * *or_out and the count of nonzero words into *n_bad (either may be NULL);
  * clear = 1 zeroes them.  Waits for the stream of the last call. */
 int gitm_hz_status(GitmVertCtx* ctx, uint32_t* or_out, int64_t* n_bad, int clear);

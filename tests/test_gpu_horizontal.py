@@ -110,3 +110,59 @@ def test_hz_rejects_large_blocks(ctx):
     b = H.synthetic_blocks(17, 16, 2, 1, 1, seed=15).to_device()
     with pytest.raises(V.GitmError):
         H.advance_horizontal(ctx, b, 2.0)
+
+
+# ---------------------------------------------------------------- exchange
+@pytest.mark.parametrize("cfg", [dict(shape=(9, 9, 10, 4, 2)), dict(shape=(5, 7, 6, 6, 3)),
+                                 dict(shape=(4, 4, 5, 2, 2), use_ion_advection=False),
+                                 dict(shape=(6, 5, 4, 4, 2), non_magnetic=True),
+                                 dict(shape=(5, 5, 3, 4, 3), north_pole=False, south_pole=False)])
+def test_exchange_matches_oracle(ctx, cfg):
+    """gitm_hz_exchange against the block-by-block restatement, bit for bit
+    (copies and sign changes only)."""
+    from oracle import hz_exchange as X
+    nl, nt, na, nbl, nbt = cfg["shape"]
+    flags = {k: v for k, v in cfg.items() if k != "shape"}
+    b = H.synthetic_blocks(nl, nt, na, nbl, nbt, seed=20 + nl)
+    ref = b.copy()
+    X.exchange(ref.arrays, nl, nt, na, nbl, nbt, **flags)
+    d = b.to_device()
+    H.exchange_messages(ctx, d, **flags)
+    got = d.to_numpy()
+    for k in ("rho", "temperature", "itemperature", "etemperature", "velocity", "vert_vel", "ndensity_s",
+              "idensity_s", "ivelocity", "ivelocity_par"):
+        np.testing.assert_array_equal(got[k], ref.arrays[k], err_msg=k)
+
+
+def test_exchange_then_advance_then_exchange(ctx, oracle_lib):
+    """advance_horizontal_all's sequence (exchange, advance, exchange) on the
+    GPU against the restatements."""
+    from oracle import hz_exchange as X
+    nl, nt, na, nbl, nbt = 9, 9, 8, 4, 2
+    b = H.synthetic_blocks(nl, nt, na, nbl, nbt, seed=30)
+    p = abi.default_hz_params()
+    ref = b.copy()
+    X.exchange(ref.arrays, nl, nt, na, nbl, nbt)
+    assert (oracle_lib.hz_advance(ref, p, 2.0) == 0).all()
+    X.exchange(ref.arrays, nl, nt, na, nbl, nbt)
+    d = b.to_device()
+    H.exchange_messages(ctx, d)
+    H.advance_horizontal(ctx, d, 2.0, p)
+    H.exchange_messages(ctx, d)
+    _compare(d.to_numpy(), ref.arrays)
+
+
+def test_exchange_reports_low_temperature(ctx):
+    from gitm_b200 import vertical as V
+    b = H.synthetic_blocks(5, 5, 3, 4, 2, seed=31)
+    b.arrays["temperature"][3, 2, 3, 3] = 50.0
+    d = b.to_device()
+    with pytest.raises(V.GitmStop):
+        H.exchange_messages(ctx, d)
+
+
+def test_exchange_rejects_odd_block_rows_with_poles(ctx):
+    from gitm_b200 import vertical as V
+    b = H.synthetic_blocks(5, 5, 3, 3, 2, seed=32).to_device()
+    with pytest.raises(V.GitmError):
+        H.exchange_messages(ctx, b)

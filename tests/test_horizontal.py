@@ -95,3 +95,70 @@ def test_oracle_variants_change_the_result(oracle_lib, variant):
     oracle_lib.hz_advance(a1, abi.default_hz_params(**variant), 2.0)
     diff = max(np.abs(a0.arrays[k] - a1.arrays[k]).max() for k in ("velocity", "idensity_s", "temperature"))
     assert diff > 0.0
+
+
+# ---------------------------------------------------------------- exchange
+def _global_source(b, i, j, nl, nt, nbl, nbt):
+    """The interior cell (block, i, j) a ghost cell covers on a sphere with
+    both poles connected: periodic in longitude, mirrored in latitude across a
+    pole with the longitude moved by nbl / 2 blocks."""
+    bx, by = b % nbl, b // nbl
+    G, GJ = bx * nl + i, by * nt + j
+    NLON, NLAT = nl * nbl, nt * nbt
+    flip = False
+    if GJ < 1:
+        GJ, G, flip = 1 - GJ, G + (nbl // 2) * nl, True
+    elif GJ > NLAT:
+        GJ, G, flip = 2 * NLAT + 1 - GJ, G + (nbl // 2) * nl, True
+    G = (G - 1) % NLON + 1
+    sbx, sby = (G - 1) // nl, (GJ - 1) // nt
+    return sby * nbl + sbx, G - sbx * nl, GJ - sby * nt, flip
+
+
+def test_exchange_oracle_follows_the_sphere():
+    """Every ghost cell of altitudes 1..nAlts holds the interior cell it
+    covers; winds and ion velocities change sign across the poles."""
+    from oracle import hz_exchange as X
+    nl, nt, na, nbl, nbt = 5, 4, 3, 4, 3
+    b0 = H.synthetic_blocks(nl, nt, na, nbl, nbt, seed=9)
+    b = b0.copy()
+    st = X.exchange(b.arrays, nl, nt, na, nbl, nbt)
+    assert (st == 0).all()
+    A, A0 = b.arrays, b0.arrays
+    for blk in range(nbl * nbt):
+        for j in range(-1, nt + 3):
+            for i in range(-1, nl + 3):
+                if 1 <= i <= nl and 1 <= j <= nt:
+                    continue
+                sb, si, sj, flip = _global_source(blk, i, j, nl, nt, nbl, nbt)
+                for k in range(1, na + 1):
+                    assert A["rho"][blk, k + 1, j + 1, i + 1] == A0["rho"][sb, k + 1, sj + 1, si + 1]
+                    for d in range(3):
+                        sign = -1.0 if (flip and d < 2) else 1.0
+                        assert A["velocity"][blk, d, k + 1, j + 1, i + 1] == \
+                            sign * A0["velocity"][sb, d, k + 1, sj + 1, si + 1]
+                        assert A["ivelocity_par"][blk, d, k + 1, j + 1, i + 1] == \
+                            sign * A0["ivelocity_par"][sb, d, k + 1, sj + 1, si + 1]
+                    for s in range(10):
+                        assert A["idensity_s"][blk, s, k + 1, j + 1, i + 1] == \
+                            A0["idensity_s"][sb, s, k + 1, sj + 1, si + 1]
+    # the polar ghost rows of the ghost altitudes are only negated (the
+    # reference's array sections run over every altitude)
+    south = A["latitude"][:, 1] < -np.pi / 2
+    np.testing.assert_array_equal(A["velocity"][south][:, 0:2, 0, 0:2], -A0["velocity"][south][:, 0:2, 0, 0:2])
+    # interiors and the fields the exchange does not move are untouched
+    np.testing.assert_array_equal(A["rho"][:, :, 2:-2, 2:-2], A0["rho"][:, :, 2:-2, 2:-2])
+    np.testing.assert_array_equal(A["gamma"], A0["gamma"])
+
+
+def test_exchange_oracle_without_poles_and_ions():
+    from oracle import hz_exchange as X
+    nl, nt, na, nbl, nbt = 4, 4, 2, 2, 2
+    b0 = H.synthetic_blocks(nl, nt, na, nbl, nbt, seed=10)
+    b = b0.copy()
+    X.exchange(b.arrays, nl, nt, na, nbl, nbt, north_pole=False, south_pole=False, use_ion_advection=False)
+    A, A0 = b.arrays, b0.arrays
+    # beyond the edges nothing moves; ions are not exchanged
+    np.testing.assert_array_equal(A["rho"][0:nbl, :, 0:2], A0["rho"][0:nbl, :, 0:2])
+    np.testing.assert_array_equal(A["idensity_s"], A0["idensity_s"])
+    assert np.abs(A["rho"] - A0["rho"]).max() > 0.0  # the east / west rings did move
