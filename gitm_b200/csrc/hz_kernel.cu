@@ -443,17 +443,34 @@ __global__ void __launch_bounds__(128) hz_exchange_kernel(const GitmHzExchange X
     const int si = int(G - int64_t(sbx) * nl), sj = int(GJ - int64_t(sby) * nt);
     const int sb = sby * X.n_blocks_lon + sbx;
     const int64_t sc = int64_t(sj + 1) * NI + (si + 1);
-    auto cp = [&](double* a, int f, int nf) { at(a, b, f, nf, k, c) = at(a, sb, f, nf, k, sc); };
-    cp(X.rho, 0, 1);
-    for (int d = 0; d < 3; ++d) cp(X.velocity, d, 3);
-    for (int s = 0; s < NS; ++s) cp(X.vert_vel, s, NS);
-    for (int s = 0; s < NS; ++s) cp(X.ndensity_s, s, GITM_NSPECIES_TOTAL);
-    cp(X.temperature, 0, 1);
-    if (X.itemperature) cp(X.itemperature, 0, 1);
-    if (X.etemperature) cp(X.etemperature, 0, 1);
-    if (X.use_ion_advection) {
-      for (int s = 0; s < GITM_NIONS; ++s) cp(X.idensity_s, s, GITM_NIONS);
-      for (int d = 0; d < 3; ++d) cp(VIw, d, 3);
+    // the moved fields in pack_vars_nblk's order (ModSphereInterface.f90:
+    // 395-447); every load is issued before the first store (source and
+    // destination share arrays, so interleaved pairs would serialise)
+    constexpr int NX = 1 + 3 + NS + NS + 3 + GITM_NIONS + 3;
+    auto field = [&](int q, int& f, int& nf) -> double* {
+      if (q == 0) { f = 0; nf = 1; return X.rho; }
+      if (q < 4) { f = q - 1; nf = 3; return X.velocity; }
+      if (q < 4 + NS) { f = q - 4; nf = NS; return X.vert_vel; }
+      if (q < 4 + 2 * NS) { f = q - 4 - NS; nf = GITM_NSPECIES_TOTAL; return X.ndensity_s; }
+      if (q == 4 + 2 * NS) { f = 0; nf = 1; return X.temperature; }
+      if (q == 5 + 2 * NS) { f = 0; nf = 1; return X.itemperature; }
+      if (q == 6 + 2 * NS) { f = 0; nf = 1; return X.etemperature; }
+      if (q < 7 + 2 * NS + GITM_NIONS) { f = q - 7 - 2 * NS; nf = GITM_NIONS; return X.use_ion_advection ? X.idensity_s : nullptr; }
+      f = q - 7 - 2 * NS - GITM_NIONS; nf = 3;
+      return X.use_ion_advection ? VIw : nullptr;
+    };
+    double v[NX];
+#pragma unroll
+    for (int q = 0; q < NX; ++q) {
+      int f, nf;
+      double* a = field(q, f, nf);
+      v[q] = a ? at(a, sb, f, nf, k, sc) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < NX; ++q) {
+      int f, nf;
+      double* a = field(q, f, nf);
+      if (a) at(a, b, f, nf, k, c) = v[q];
     }
   }
   __syncthreads();
