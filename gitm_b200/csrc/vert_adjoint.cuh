@@ -1026,6 +1026,8 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       c.gm(i) = gamma;
       if (i == -1) c.sc(SC_MMM_M1) = mmm;
       if (i == 0) c.sc(SC_MMM_0) = mmm;
+      // with saved stage states the state itself comes from them
+      if (kp.saved) continue;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         c.x(F_LNS + s, i) = log(nd[s]);

@@ -97,14 +97,15 @@ __device__ __forceinline__ bool in_pcells(int i, int nAlts) {
 
 __device__ __forceinline__ bool photochemical(int s) { return s == 3 || s == 4; }  // N(4S), NO
 
-// ModLimiter.f90:16-36
+// ModLimiter.f90:16-36, without branches: both candidates are formed and
+// the signs select one (the same values as the reference's if-blocks; lanes
+// whose cells take different cases do not split the warp)
 __device__ __forceinline__ double limiter_mc(double u, double d, double beta) {
-  if (u > 0.0) {
-    if (d > 0.0) return fmin(fmin(beta * u, beta * d), (u + d) * 0.5);
-    return 0.0;
-  }
-  if (d < 0.0) return fmax(fmax(beta * u, beta * d), (u + d) * 0.5);
-  return 0.0;
+  const double bu = beta * u, bd = beta * d, av = (u + d) * 0.5;
+  const double lo = fmin(fmin(bu, bd), av), hi = fmax(fmax(bu, bd), av);
+  const bool pos = (u > 0.0) && (d > 0.0);
+  const bool neg = !(u > 0.0) && (d < 0.0);
+  return pos ? lo : (neg ? hi : 0.0);
 }
 
 struct ColCtx {
