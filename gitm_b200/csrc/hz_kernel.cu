@@ -56,14 +56,15 @@ __host__ __device__ inline HzLayout hz_layout(int nLons, int nLats) {
   return L;
 }
 
-// Limiter_mc (ModLimiter.f90:16-36)
+// Limiter_mc (ModLimiter.f90:16-36) without branches: both candidates are
+// formed and the signs select one, so lanes of different cases do not split
+// the warp
 __device__ __forceinline__ double hz_limiter(double u, double d, double beta) {
-  if (u > 0.0) {
-    if (d > 0.0) return fmin(fmin(beta * u, beta * d), (u + d) * 0.5);
-    return 0.0;
-  }
-  if (d < 0.0) return fmax(fmax(beta * u, beta * d), (u + d) * 0.5);
-  return 0.0;
+  const double bu = beta * u, bd = beta * d, av = (u + d) * 0.5;
+  const double lo = fmin(fmin(bu, bd), av), hi = fmax(fmax(bu, bd), av);
+  const bool pos = (u > 0.0) && (d > 0.0);
+  const bool neg = !(u > 0.0) && (d < 0.0);
+  return pos ? lo : (neg ? hi : 0.0);
 }
 
 // The limited slope of line cell q (0 .. n+1) as calc_facevalues_lons /

@@ -89,12 +89,11 @@ struct AParams {
 // beta ob (1) or ob / 2 (3), and d beta ob (2) or ob / 2 (3).
 __device__ __forceinline__ int limiter_mc_branch(double u, double d, double beta) {
   const double bu = beta * u, bd = beta * d, av = (u + d) * 0.5;
-  if (u > 0.0) {
-    if (d > 0.0) return (fmin(bu, bd) <= av) ? ((bu <= bd) ? 1 : 2) : 3;
-    return 0;
-  }
-  if (d < 0.0) return (fmax(bu, bd) >= av) ? ((bu >= bd) ? 1 : 2) : 3;
-  return 0;
+  const bool pos = (u > 0.0) && (d > 0.0);
+  const bool neg = !(u > 0.0) && (d < 0.0);
+  const int cp = (fmin(bu, bd) <= av) ? ((bu <= bd) ? 1 : 2) : 3;
+  const int cn = (fmax(bu, bd) >= av) ? ((bu >= bd) ? 1 : 2) : 3;
+  return pos ? cp : (neg ? cn : 0);
 }
 
 // Per-column view of the adjoint arrays in shared memory.
