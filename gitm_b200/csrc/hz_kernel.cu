@@ -74,19 +74,14 @@ __device__ __forceinline__ double hz_slope(const double* V, const double* IF, in
                                            double beta) {
   auto v = [&](int x) { return V[(x + 1) * s]; };
   auto f = [&](int x) { return IF[(x + 1) * s]; };
-  double up, dn;
-  if (q == n + 1) {
-    up = (v(q + 1) - v(q)) * f(q + 1);
-  } else {
-    const double h = f(q + 1) * 2;
-    up = h * (F1 * (v(q + 1) - v(q)) - F2 * (v(q + 2) - v(q - 1)));
-  }
-  if (q == 0) {
-    dn = (v(q) - v(q - 1)) * f(q);
-  } else {
-    const double h = f(q) * 2;
-    dn = h * (F1 * (v(q) - v(q - 1)) - F2 * (v(q + 1) - v(q - 2)));
-  }
+  // both forms in one expression: the 2nd-order side is h * (1 * (...) -
+  // 0 * (...)) with h = IF, exactly; the outer neighbours are clamped into
+  // the line (finite values the zero factor removes)
+  const bool eu = (q == n + 1), ed = (q == 0);
+  const double hu = eu ? f(q + 1) : f(q + 1) * 2, hd = ed ? f(q) : f(q) * 2;
+  const double au = eu ? 1.0 : F1, bu = eu ? 0.0 : F2, ad = ed ? 1.0 : F1, bd = ed ? 0.0 : F2;
+  const double up = hu * (au * (v(q + 1) - v(q)) - bu * (v(min(q + 2, n + 2)) - v(q - 1)));
+  const double dn = hd * (ad * (v(q) - v(q - 1)) - bd * (v(q + 1) - v(max(q - 2, -1))));
   return hz_limiter(up, dn, beta);
 }
 

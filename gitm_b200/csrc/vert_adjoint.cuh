@@ -774,17 +774,14 @@ __device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, in
   const bool end = (i == 0 || i == nA + 1);
   const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
   const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
+  // both forms in one expression, as rusanov_slopes_cell
+  const double fa = end ? 1.0 : F1, fb = end ? 0.0 : F2;
+  const int ip2 = min(i + 2, nA + 2), im2 = max(i - 2, -1);
 #pragma unroll 3
   for (int f = 0; f < NSTENCIL; ++f) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
-    double u, d;
-    if (end) {
-      u = (v[i + 1] - v[i]) * cu;
-      d = (v[i] - v[i - 1]) * cd;
-    } else {
-      u = cu * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-      d = cd * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-    }
+    const double u = cu * (fa * (v[i + 1] - v[i]) - fb * (v[ip2] - v[i - 1]));
+    const double d = cd * (fa * (v[i] - v[i - 1]) - fb * (v[i + 1] - v[im2]));
     c.dl(f, i) = limiter_mc(u, d, beta);
     a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(u, d, beta));
   }

@@ -593,20 +593,20 @@ __device__ __forceinline__ void rusanov_cell(ColCtx c, int i, const GitmVertPara
 // cell diverges only over the two differences (threads over cells
 // 0..nAlts+1 of every column).
 __device__ __forceinline__ void rusanov_slopes_cell(ColCtx c, int i, double beta) {
-  const bool end = (i == 0 || i == c.L.nAlts + 1);
+  const int nA = c.L.nAlts;
+  const bool end = (i == 0 || i == nA + 1);
   const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
   const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
+  // one expression for both forms: the end cells' 2nd-order differences are
+  // cu * (1 * (v[i+1] - v[i]) - 0 * (...)), exactly; their outer neighbours
+  // are clamped into the column (finite values the zero factor removes)
+  const double a = end ? 1.0 : F1, b = end ? 0.0 : F2;
+  const int ip2 = min(i + 2, nA + 2), im2 = max(i - 2, -1);
 #pragma unroll 3
   for (int f = 0; f < NSTENCIL; ++f) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
-    double u, d;
-    if (end) {
-      u = (v[i + 1] - v[i]) * cu;
-      d = (v[i] - v[i - 1]) * cd;
-    } else {
-      u = cu * (F1 * (v[i + 1] - v[i]) - F2 * (v[i + 2] - v[i - 1]));
-      d = cd * (F1 * (v[i] - v[i - 1]) - F2 * (v[i + 1] - v[i - 2]));
-    }
+    const double u = cu * (a * (v[i + 1] - v[i]) - b * (v[ip2] - v[i - 1]));
+    const double d = cd * (a * (v[i] - v[i - 1]) - b * (v[i + 1] - v[im2]));
     c.dl(f, i) = limiter_mc(u, d, beta);
   }
 }
