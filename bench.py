@@ -492,10 +492,44 @@ def run_adjoint(args):
     t_plain = f0.elapsed_time(f1) / 1e3
     free0 = torch.cuda.mem_get_info(dev)[0]
     torch.cuda.reset_peak_memory_stats(dev)
-    grads, t_fwd, t_bwd, Jv = grads_once(args.adj_steps)
+    # three timed rollouts, the median of each leg (the backward runs from
+    # Python autograd, so host load on the machine shows in single runs)
+    runs = [grads_once(args.adj_steps) for _ in range(3)]
+    grads, _, _, Jv = runs[-1]
+    t_fwd = statistics.median(r[1] for r in runs)
+    t_bwd = statistics.median(r[2] for r in runs)
     peak_torch = torch.cuda.max_memory_allocated(dev)
     free1 = torch.cuda.mem_get_info(dev)[0]
     run.check()
+    # device time of one backward step's two launches in a tight loop: the
+    # saving step kernel and the adjoint kernel on fixed buffers
+    sbuf = run.saved_buffer()
+    st0 = {k: v.clone() for k, v in base.items()}
+    ybar = {k: torch.ones_like(v) for k, v in base.items()}
+    for _ in range(2):
+        run.step_saving(st0, sbuf, eddy0, hs0)
+        run.vjp(st0, ybar, eddy0, hs0, saved=sbuf)
+    n_k = 10
+    t_save = t_adj = 0.0
+    for _ in range(n_k):
+        a0, a1, a2, a3 = ev(), ev(), ev(), ev()
+        run._load(st0, eddy0, hs0)
+        a0.record()
+        run.plan.advance_saving(DT, sbuf)
+        a1.record()
+        bars = {k: ybar[k].clone() for k in ybar}
+        bars["eddy"] = torch.zeros_like(eddy0)
+        bars["heating_scale"] = torch.zeros_like(hs0)
+        run._load(st0, eddy0, hs0)
+        a2.record()
+        run.plan.adjoint([bars], DT, saved=sbuf)
+        a3.record()
+        a3.synchronize()
+        t_save += a0.elapsed_time(a1) / 1e3
+        t_adj += a2.elapsed_time(a3) / 1e3
+    t_save /= n_k
+    t_adj /= n_k
+    del sbuf
 
     # finite differences: directions on one column each, eps = 1e-7 relative,
     # over one step and over the whole rollout; no direction is filtered out,
@@ -559,6 +593,10 @@ def run_adjoint(args):
                "forward_plain_ms_per_step": 1e3 * t_plain / n,
                "forward_checkpointed_ms_per_step": 1e3 * t_fwd / n,
                "backward_ms_per_step": 1e3 * t_bwd / n,
+               "backward_device_ms_per_step": {"saving_step": 1e3 * t_save, "adjoint_kernel": 1e3 * t_adj,
+                                               "how": "the two launches of a backward step on fixed buffers, "
+                                                      "CUDA events around each, mean of 10"},
+               "timing": "median of 3 timed rollouts",
                "backward_includes": "segment recompute (the step kernel saving its stage states) + one adjoint "
                                     "kernel per step reading them",
                "objective_value": Jv,

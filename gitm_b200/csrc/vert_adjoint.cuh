@@ -796,23 +796,21 @@ __device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, d
   // the 4th-order differences with the mesh factors cu, cd
   const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
   const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
+  const double fa = end ? 1.0 : F1, fb = end ? 0.0 : F2;
+  const int ip2 = min(i + 2, nA + 2), im2 = max(i - 2, -1);
   for (int f = 0; f < NSTENCIL; ++f) {
     const double ob = a.db[f * (nA + 2) + i];
     const int br = a.lc[f * (nA + 2) + i];
     if (ob == 0.0 || br == 0) continue;
     const double ub = (br == 1) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
     const double dbv = (br == 2) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
-    if (end) {
-      a.add(f, i + 1, cu * ub);
-      a.add(f, i, -cu * ub + cd * dbv);
-      a.add(f, i - 1, -cd * dbv);
-    } else {
-      a.add(f, i + 2, -cu * F2 * ub);
-      a.add(f, i + 1, cu * F1 * ub - cd * F2 * dbv);
-      a.add(f, i, -cu * F1 * ub + cd * F1 * dbv);
-      a.add(f, i - 1, cu * F2 * ub - cd * F1 * dbv);
-      a.add(f, i - 2, cd * F2 * dbv);
-    }
+    // one form for both kinds of cell (fa = 1, fb = 0 at the ends): the
+    // end cells add zeros to their clamped outer neighbours
+    a.add(f, ip2, -cu * fb * ub);
+    a.add(f, i + 1, cu * fa * ub - cd * fb * dbv);
+    a.add(f, i, -cu * fa * ub + cd * fa * dbv);
+    a.add(f, i - 1, cu * fb * ub - cd * fa * dbv);
+    a.add(f, im2, cd * fb * dbv);
   }
 }
 
