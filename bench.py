@@ -465,13 +465,13 @@ def run_adjoint(args):
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    def grads_once(n_steps):
+    def grads_once(n_steps, every=None):
         s0 = {k: v.clone().requires_grad_(True) for k, v in base.items()}
         ed = eddy0.clone().requires_grad_(True)
         hs = hs0.clone().requires_grad_(True)
         e0, e1, e2 = ev(), ev(), ev()
         e0.record()
-        out = AD.rollout(run, s0, n_steps, args.adj_every, ed, hs)
+        out = AD.rollout(run, s0, n_steps, args.adj_every if every is None else every, ed, hs)
         J = AD.o_n2_objective(out["ndensity_s"], w, lvl)
         e1.record()
         g = torch.autograd.grad(J, [s0[k] for k in names] + [ed, hs])
@@ -500,6 +500,26 @@ def run_adjoint(args):
     t_bwd = statistics.median(r[2] for r in runs)
     peak_torch = torch.cuda.max_memory_allocated(dev)
     free1 = torch.cuda.mem_get_info(dev)[0]
+    # the same rollout keeping every step's stage states from the forward
+    # (every = 0: no recompute in the backward), where they fit
+    kept = None
+    if args.adj_steps * run.stage_bytes_per_step() < 0.8 * free1:
+        grads_once(args.adj_steps, every=0)
+        torch.cuda.reset_peak_memory_stats(dev)
+        runs0 = [grads_once(args.adj_steps, every=0) for _ in range(3)]
+        k_fwd = statistics.median(r[1] for r in runs0)
+        k_bwd = statistics.median(r[2] for r in runs0)
+        g0 = runs0[-1][0]
+        agree = max(float((a - b).norm() / max(float(b.norm()), 1e-300)) for a, b in zip(g0, grads))
+        kept = {"forward_ms_per_step": 1e3 * k_fwd / args.adj_steps,
+                "backward_ms_per_step": 1e3 * k_bwd / args.adj_steps,
+                "backward_over_forward_plain": k_bwd / t_plain,
+                "peak_torch_allocated_bytes": int(torch.cuda.max_memory_allocated(dev)),
+                "max_rel_diff_vs_checkpointed_gradient": agree,
+                "how": "rollout(every = 0): the forward steps with the saving step kernel and keeps each "
+                       "step's input and stage states; the backward runs the adjoint kernels only; "
+                       "median of 3 timed rollouts"}
+        del runs0, g0
     run.check()
     # device time of one backward step's two launches in a tight loop: the
     # saving step kernel and the adjoint kernel on fixed buffers
@@ -597,6 +617,7 @@ def run_adjoint(args):
                                                "how": "the two launches of a backward step on fixed buffers, "
                                                       "CUDA events around each, mean of 10"},
                "timing": "median of 3 timed rollouts",
+               "stages_kept": kept,
                "backward_includes": "segment recompute (the step kernel saving its stage states) + one adjoint "
                                     "kernel per step reading them",
                "objective_value": Jv,

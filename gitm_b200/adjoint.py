@@ -13,7 +13,9 @@ sensitivity studies and data assimilation:
   ``n_steps`` rollout that keeps only every ``every``-th state in memory and
   recomputes the states of a segment when its adjoint runs (checkpointing);
   the recompute saves each step's stage states (``step_saving``) and the
-  adjoint kernel reads them.
+  adjoint kernel reads them.  ``every = 0`` keeps every step's input state
+  and stage states from the forward itself (no recompute: about seven
+  states of memory per step, ``stage_bytes_per_step``).
 * ``o_n2_objective`` is the column-weighted log(n_O / n_N2) at one altitude
   level.
 
@@ -81,6 +83,22 @@ class StepRunner:
         self.plan.advance_saving(self.dt, saved)
         return self.state()
 
+    def stage_bytes_per_step(self) -> int:
+        """Device bytes one step keeps when a rollout keeps its stages: the
+        saved stage states and the step's input state."""
+        n = self.plan.saved_state_doubles() + sum(self.dm.tensors[k].numel() for k in STATE)
+        return 8 * n
+
+    def vjp_into(self, state, bars, eddy_bar, hs_bar, eddy=None, heating_scale=None, saved=None):
+        """vjp() in place: `bars` holds ybar for the STATE arrays on entry and
+        xbar on return (contiguous float64 CUDA tensors); eddy_bar / hs_bar
+        (may be None) accumulate."""
+        self._load(state, eddy, heating_scale)
+        b = dict(bars)
+        b["eddy"] = eddy_bar
+        b["heating_scale"] = hs_bar if self.dm.tensors.get("heating_scale") is not None else None
+        self.plan.adjoint([b], self.dt, saved=saved)
+
     def vjp(self, state, ybar, eddy=None, heating_scale=None, saved=None):
         """Adjoint of one step taken from `state`: returns (xbar, eddy_bar,
         heating_scale_bar).  ybar: dict of output adjoints (None = zero);
@@ -138,12 +156,25 @@ class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, runner, n_steps, every, eddy, heating_scale, *state):
         s = dict(zip(STATE, (t.detach() for t in state)))
-        ckpts = []
+        ckpts, stages = [], []
+        if every == 0:
+            need = n_steps * runner.stage_bytes_per_step()
+            free = torch.cuda.mem_get_info(runner.tensors["rho"].device)[0]
+            if need > 0.9 * free:
+                raise V.GitmError(f"rollout with every = 0 keeps {need / 1e9:.1f} GB of stage states, "
+                                  f"{free / 1e9:.1f} GB free: use checkpoints (every > 0)")
+            s = {k: v.clone() for k, v in s.items()}
         for t in range(n_steps):
+            if every == 0:
+                # keep the step's input and its stage states
+                buf = runner.saved_buffer()
+                stages.append((s, buf))
+                s = runner.step_saving(s, buf, eddy, heating_scale)
+                continue
             if t % every == 0:
                 ckpts.append({k: v.clone() for k, v in s.items()})
             s = runner.step(s, eddy, heating_scale)
-        ctx.runner, ctx.n_steps, ctx.every, ctx.ckpts = runner, n_steps, every, ckpts
+        ctx.runner, ctx.n_steps, ctx.every, ctx.ckpts, ctx.stages = runner, n_steps, every, ckpts, stages
         ctx.save_for_backward(eddy, heating_scale)
         return tuple(s[k] for k in STATE)
 
@@ -151,40 +182,50 @@ class _Rollout(torch.autograd.Function):
     def backward(ctx, *ybar):
         eddy, hs = ctx.saved_tensors
         runner = ctx.runner
-        y = dict(zip(STATE, ybar))
-        eb = torch.zeros_like(eddy)
-        hb = torch.zeros_like(hs)
+        # the running adjoint, updated in place step by step
+        y = {k: (torch.zeros_like(runner.tensors[k]) if g is None else g.detach().clone().contiguous())
+             for k, g in zip(STATE, ybar)}
+        eb = torch.zeros_like(runner.tensors["eddy"])
+        hrun = runner.tensors.get("heating_scale")
+        hb = None if hrun is None else torch.zeros_like(hrun)
         n, k = ctx.n_steps, ctx.every
-        saved = []  # one stage-state buffer per step of a segment, reused
-        for seg in reversed(range(len(ctx.ckpts))):
-            t0 = seg * k
-            t1 = min(t0 + k, n)
-            # recompute the segment's step inputs, saving each step's stages
-            states = [ctx.ckpts[seg]]
-            while len(saved) < t1 - t0:
-                saved.append(runner.saved_buffer())
-            for j in range(t1 - t0):
-                nxt = runner.step_saving(states[-1], saved[j], eddy, hs)
-                if j < t1 - t0 - 1:
-                    states.append(nxt)
-            for j in reversed(range(t1 - t0)):
-                y, e, h = runner.vjp(states[j], y, eddy, hs, saved=saved[j])
-                eb += e
-                if h is not None and hb.shape == h.shape:
-                    hb += h
-            ctx.ckpts[seg] = None
+        if k == 0:
+            for j in reversed(range(n)):
+                st, buf = ctx.stages[j]
+                runner.vjp_into(st, y, eb, hb, eddy, hs, saved=buf)
+                ctx.stages[j] = None
+        else:
+            saved = []  # one stage-state buffer per step of a segment, reused
+            for seg in reversed(range(len(ctx.ckpts))):
+                t0 = seg * k
+                t1 = min(t0 + k, n)
+                # recompute the segment's step inputs, saving each step's stages
+                states = [ctx.ckpts[seg]]
+                while len(saved) < t1 - t0:
+                    saved.append(runner.saved_buffer())
+                for j in range(t1 - t0):
+                    nxt = runner.step_saving(states[-1], saved[j], eddy, hs)
+                    if j < t1 - t0 - 1:
+                        states.append(nxt)
+                for j in reversed(range(t1 - t0)):
+                    runner.vjp_into(states[j], y, eb, hb, eddy, hs, saved=saved[j])
+                ctx.ckpts[seg] = None
+        eb = eb.reshape(eddy.shape)
+        if hb is None or hb.shape != hs.shape:
+            hb = torch.zeros_like(hs)
         return (None, None, None, eb, hb, *[y[k2] for k2 in STATE])
 
 
 def rollout(runner: StepRunner, state: dict, n_steps: int, every: int = 10, eddy=None,
             heating_scale=None) -> dict:
-    """n_steps steps with checkpoints every `every` steps (see module doc)."""
+    """n_steps steps with checkpoints every `every` steps, or with every
+    step's stage states kept when every = 0 (see module doc)."""
     if eddy is None:
         eddy = runner.tensors["eddy"].clone()
     if heating_scale is None:
         hs = runner.tensors.get("heating_scale")
         heating_scale = torch.ones(1, device=eddy.device, dtype=eddy.dtype) if hs is None else hs.clone()
-    out = _Rollout.apply(runner, int(n_steps), max(1, int(every)), eddy, heating_scale,
+    out = _Rollout.apply(runner, int(n_steps), max(0, int(every)), eddy, heating_scale,
                          *[state[k] for k in STATE])
     return dict(zip(STATE, out))
 

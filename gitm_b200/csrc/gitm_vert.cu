@@ -82,7 +82,9 @@ struct GitmVertPlan {
   size_t adj_scratch_per_cta = 0;
   double* d_adj_scratch = nullptr;
   GitmColumnAdjoint* d_bars = nullptr;
-  // the saving step kernel (adjoint tiles, its own persistent grid)
+  // the saving step kernel (its own tiles and persistent grid)
+  std::vector<Tile> save_tiles;
+  Tile* d_save_tiles = nullptr;
   int save_grid = 0;
   size_t save_smem = 0;
   double* d_save_scratch = nullptr;
@@ -499,6 +501,7 @@ static int plan_common(GitmVertPlan* P, const double* const* alt, const double* 
 static void plan_free(GitmVertPlan* P) {
   if (!P) return;
   cudaFree(P->d_adj_tiles);
+  cudaFree(P->d_save_tiles);
   cudaFree(P->d_adj_scratch);
   cudaFree(P->d_save_scratch);
   cudaFree(P->d_bars);
@@ -775,11 +778,22 @@ constexpr int kAdjThreads = ADJ_THREADS;
 static int adjoint_prepare(GitmVertPlan* P) {
   GitmVertCtx* ctx = P->ctx;
   if (P->adj_ready) return GITM_OK;
-  const int T = kAdjThreads;
+  const int T = kAdjThreads, TS = SAVE_THREADS;
   P->adj_tiles.clear();
+  P->save_tiles.clear();
   P->adj_smem = 0;
   P->adj_nc_max = 1;
   P->adj_per_max = 0;
+  P->save_smem = 0;
+  auto cut = [](std::vector<Tile>& out, int m, int64_t n_cols, int nc) {
+    for (int64_t c0 = 0; c0 < n_cols; c0 += nc) {
+      Tile t;
+      t.member = m;
+      t.nc = int(std::min<int64_t>(nc, n_cols - c0));
+      t.c0 = c0;
+      out.push_back(t);
+    }
+  };
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnBatch& b = P->host_members[m];
     const int nA = b.n_alts;
@@ -790,13 +804,14 @@ static int adjoint_prepare(GitmVertPlan* P) {
     P->adj_smem = std::max(P->adj_smem, adj_smem_bytes(nA, nc));
     P->adj_nc_max = std::max(P->adj_nc_max, nc);
     P->adj_per_max = std::max(P->adj_per_max, adj_state_doubles(nA));
-    for (int64_t c0 = 0; c0 < b.n_cols; c0 += nc) {
-      Tile t;
-      t.member = m;
-      t.nc = int(std::min<int64_t>(nc, b.n_cols - c0));
-      t.c0 = c0;
-      P->adj_tiles.push_back(t);
-    }
+    cut(P->adj_tiles, m, b.n_cols, nc);
+    // the saving step kernel: columns per CTA of the forward layout
+    int ns = std::max(1, std::min(TS / nA, TS / 32));
+    while (ns > 1 && smem_bytes(nA, ns) > ctx->max_smem) --ns;
+    if (nA > TS || smem_bytes(nA, ns) > ctx->max_smem)
+      return set_err(ctx, GITM_ERR_UNSUPPORTED, "saving step: nAlts %d does not fit a CTA of %d threads", nA, TS);
+    P->save_smem = std::max(P->save_smem, smem_bytes(nA, ns));
+    cut(P->save_tiles, m, b.n_cols, ns);
   }
   if (P->adj_tiles.empty()) {
     P->adj_ready = true;
@@ -817,17 +832,17 @@ static int adjoint_prepare(GitmVertPlan* P) {
     return set_err(ctx, GITM_ERR_NOMEM, "adjoint: cannot allocate the stage-state scratch");
   }
   CUDA_TRY(ctx, cudaMalloc(&P->d_bars, std::max(1, P->n_members) * sizeof(GitmColumnAdjoint)));
-  // the saving step kernel runs on the same tiles with the forward layout
+  // the saving step kernel: its own tiles, the forward layout
   const void* sfn = saving_kernel_fn();
   CUDA_TRY(ctx, cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem)));
-  P->save_smem = 0;
-  for (const Tile& t : P->adj_tiles)
-    P->save_smem = std::max(P->save_smem, smem_bytes(P->host_members[t.member].n_alts, t.nc));
   int sper = 0;
-  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, sfn, T, P->save_smem));
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, sfn, TS, P->save_smem));
   sper = std::max(sper, 1);
-  P->save_grid = int(std::min<size_t>(P->adj_tiles.size(), size_t(sper) * ctx->num_sms));
-  if (cudaMalloc(&P->d_save_scratch, size_t(P->save_grid) * NF * T * sizeof(double)) != cudaSuccess) {
+  P->save_grid = int(std::min<size_t>(P->save_tiles.size(), size_t(sper) * ctx->num_sms));
+  CUDA_TRY(ctx, cudaMalloc(&P->d_save_tiles, P->save_tiles.size() * sizeof(Tile)));
+  CUDA_TRY(ctx, cudaMemcpy(P->d_save_tiles, P->save_tiles.data(), P->save_tiles.size() * sizeof(Tile),
+                           cudaMemcpyHostToDevice));
+  if (cudaMalloc(&P->d_save_scratch, size_t(P->save_grid) * NF * TS * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     return set_err(ctx, GITM_ERR_NOMEM, "adjoint: cannot allocate the saving step's scratch");
   }
@@ -866,8 +881,8 @@ extern "C" int gitm_vert_plan_advance_saving(GitmVertPlan* P, double dt, double*
   KParams kp;
   std::memset(&kp, 0, sizeof kp);
   kp.members = P->d_members;
-  kp.tiles = P->d_adj_tiles;
-  kp.n_tiles = int(P->adj_tiles.size());
+  kp.tiles = P->d_save_tiles;
+  kp.n_tiles = int(P->save_tiles.size());
   kp.n_steps = 1;
   kp.dt = dt;
   kp.status = P->d_status;
@@ -877,7 +892,7 @@ extern "C" int gitm_vert_plan_advance_saving(GitmVertPlan* P, double dt, double*
   kp.save_ncols = P->n_cols_total;
   kp.save_per = P->adj_per_max;
   void* args[] = {&kp};
-  CUDA_TRY(ctx, cudaLaunchKernel(saving_kernel_fn(), dim3(P->save_grid), dim3(ADJ_THREADS), args, P->save_smem,
+  CUDA_TRY(ctx, cudaLaunchKernel(saving_kernel_fn(), dim3(P->save_grid), dim3(SAVE_THREADS), args, P->save_smem,
                                  static_cast<cudaStream_t>(stream)));
   return GITM_OK;
 }

@@ -50,7 +50,10 @@ __host__ __device__ inline size_t adj_smem_bytes(int nAlts, int nc) {
 }
 
 constexpr int ADJ_NSTATE = 6;    // gathered state, X0, X1, X2, X3, X4
-constexpr int ADJ_THREADS = 128;  // threads per CTA of the adjoint kernel
+// threads per CTA of the adjoint kernel (2 columns of 50 cells per CTA; 64
+// threads with one column measured 3 % slower) and of the saving step kernel
+constexpr int ADJ_THREADS = 128;
+constexpr int SAVE_THREADS = 128;
 
 // Defined in vert_adjoint.cu (the kernel's own translation unit).
 const void* adjoint_kernel_fn();
@@ -1180,6 +1183,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
 
     const double wk[4] = {1.0, 2.0, 2.0, 1.0};
     const double ck[3] = {0.5, 0.5, 1.0};
+    double eddy_bar = 0.0;  // the four stages' KappaEddyDiffusion adjoints of this thread's cell
     for (int k = 3; k >= 0; --k) {
       load(1 + k, L.X0);
       for (int cl = 0; cl < nc; ++cl) {
@@ -1195,12 +1199,11 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       if (item) {
         ColCtx c = ctx(my_cl);
         ColAdj a = adj(my_cl);
-        const double eb = cell_adjoint_species(c, a, my_i, prm, dt, eddy, kbs, NT);
+        eddy_bar += cell_adjoint_species(c, a, my_i, prm, dt, eddy, kbs, NT);
         cell_adjoint_rest(c, a, my_i, dt, ivup, kbs, NT);
         // K = New - state: the state's own -K
 #pragma unroll
         for (int f = 0; f < NF; ++f) a.add(f, my_i, -kbs[size_t(f) * NT]);
-        if (B.eddy && !sfrozen[my_cl]) B.eddy[gidx(0, my_i + 1, my_cl)] += eb;
       }
       __syncthreads();  // @phase 9
       for (int j = tid; j < nc * (nA + 2); j += NT) {
@@ -1232,17 +1235,26 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       }
     }
 
+    if (item && B.eddy && !sfrozen[my_cl]) B.eddy[gidx(0, my_i + 1, my_cl)] += eddy_bar;
+
     // ------------------------------------------------------------ gather^T
     for (int w = tid; w < nc * G; w += NT) {
       const int g = w / nc, cl = w - g * nc, i = g - 1;
       if (sfrozen[cl]) continue;
       ColCtx c = ctx(cl);
       ColAdj a = adj(cl);
+      // the step's inputs and the adjoint arrays do not overlap: restrict
+      // lets the loads of one cell be issued ahead of its stores
+      const double* __restrict__ in_nd = b.ndensity_s;
+      const double* __restrict__ in_ww = b.vert_vel;
+      const double* __restrict__ in_rho = b.rho;
+      const double* __restrict__ in_ion = b.idensity_s;
+      double* __restrict__ out_ion = B.idensity_s;
       double nd[NS], ww[NS], ndb[NS], wwb[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        nd[s] = b.ndensity_s[gidx(s, g, cl)];
-        ww[s] = b.vert_vel[gidx(s, g, cl)];
+        nd[s] = in_nd[gidx(s, g, cl)];
+        ww[s] = in_ww[gidx(s, g, cl)];
         ndb[s] = a.x(F_LNS + s, i) / nd[s];
         wwb[s] = a.x(F_W + s, i);
       }
@@ -1295,21 +1307,21 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       B.velocity[gidx(0, g, cl)] = a.x(F_VE, i);
       B.velocity[gidx(1, g, cl)] = a.x(F_VN, i);
       B.velocity[gidx(2, g, cl)] = a.x(F_VU, i);
-      B.rho[gidx(0, g, cl)] = a.x(F_LRHO, i) / b.rho[gidx(0, g, cl)];
+      B.rho[gidx(0, g, cl)] = a.x(F_LRHO, i) / in_rho[gidx(0, g, cl)];
       if (prm.use_ion_advection) {
         const bool improved = prm.use_improved_ion_advection != 0;
         const bool pc = in_pcells(i, nA);
-        const double ye = B.idensity_s[gidx(NI, g, cl)];
+        const double ye = out_ion[gidx(NI, g, cl)];
 #pragma unroll
         for (int s = 0; s < NI; ++s) {
           if (s < NADV || pc) {
-            const double v = b.idensity_s[gidx(s, g, cl)];
-            B.idensity_s[gidx(s, g, cl)] = improved ? a.ion(s, i) : a.ion(s, i) / v;
+            const double v = in_ion[gidx(s, g, cl)];
+            out_ion[gidx(s, g, cl)] = improved ? a.ion(s, i) : a.ion(s, i) / v;
           } else {
-            B.idensity_s[gidx(s, g, cl)] += ye;  // unchanged by the step, summed into e-
+            out_ion[gidx(s, g, cl)] += ye;  // unchanged by the step, summed into e-
           }
         }
-        B.idensity_s[gidx(NI, g, cl)] = 0.0;
+        out_ion[gidx(NI, g, cl)] = 0.0;
       }
     }
     if (tid < nc && !sfrozen[tid] && b.heating && B.heating_scale)

@@ -113,7 +113,9 @@ def test_adjoint_matches_autograd(cuda, variant):
         assert _rel(g, w) < 1e-9, (k, _rel(g, w))
 
 
-def test_rollout_equals_stepwise_composition(cuda):
+@pytest.mark.parametrize("every", [2, 0])
+def test_rollout_equals_stepwise_composition(cuda, every):
+    """Checkpoints every 2 steps, and every step's stages kept (every = 0)."""
     from gitm_b200 import adjoint as AD
     from gitm_b200 import vertical as V
     p = abi.default_params()
@@ -125,7 +127,7 @@ def test_rollout_equals_stepwise_composition(cuda):
     hs = run.tensors["heating_scale"].clone().requires_grad_(True)
     w = torch.rand(32, dtype=torch.float64, device=cuda, generator=torch.Generator(cuda).manual_seed(1))
     lvl = AD.level_of(m.altitude, 400e3)
-    out = AD.rollout(run, s0, 6, 2, eddy, hs)
+    out = AD.rollout(run, s0, 6, every, eddy, hs)
     g1 = torch.autograd.grad(AD.o_n2_objective(out["ndensity_s"], w, lvl), [s0["ndensity_s"], s0["temperature"],
                                                                                  s0["velocity"], eddy, hs])
     s = s0
