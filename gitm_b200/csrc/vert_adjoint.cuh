@@ -544,12 +544,13 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
 #pragma unroll
   for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
   const double ir = exp(-LR);
-  // reverse of New LogRho = log(sumrho): the continuity adjoints
+  // reverse of New LogRho = log(sumrho): the continuity adjoints, with
+  // New LogNS's own adjoint (read here, before the first shared atomic)
   double nlb[NS];
   {
     const double srb = kb(F_LRHO) / sumrho;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) nlb[s] = srb * menl[s];
+    for (int s = 0; s < NS; ++s) nlb[s] = srb * menl[s] + kb(F_LNS + s);
   }
   double Tb = 0.0, VEb = 0.0, VNb = 0.0, LRb = 0.0, irb = 0.0;
   double nsb[NS], wb[NS], lself[NS];  // lself: GradLogConS's share of this cell's LogNS adjoint
@@ -697,7 +698,7 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
     const double dWb = dt * w;
     corb += w;
     // New LogNS = nl = Ls - dt (divw + Ws gL) + dt dL
-    const double n = nlb[s] + kb(F_LNS + s);
+    const double n = nlb[s];
     double Lb = lself[s] + n;
     const double divwb = -dt * n;
     Wb += -dt * gL * n + 2 * invr * divwb;
@@ -729,6 +730,11 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
 __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i, double dt, double ivup,
                                          const double* kbp, int kstride) {
   auto kb = [&](int f) { return kbp[size_t(f) * kstride]; };
+  // the New adjoints this pass reads, before its first shared atomic
+  double ki[NADV];
+#pragma unroll
+  for (int s = 0; s < NADV; ++s) ki[s] = kb(F_I + s);
+  const double kE = kb(F_VE), kN = kb(F_VN), kT = kb(F_T);
   CellFaces fa(c, i);
   const double invr = c.g(GC_INVR, i);
   const double T = c.x(F_T, i), VU = c.x(F_VU, i);
@@ -742,12 +748,11 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
   // ions: New = I - dt (IVel gI) + dt dI
 #pragma unroll
   for (int s = 0; s < NADV; ++s) {
-    const double k = kb(F_I + s);
+    const double k = ki[s];
     const double own = fa.sweep_adj(c, a, F_I + s, i, -dt * ivup * k, dt * k);
     a.add(F_I + s, i, k + own);
   }
   // horizontal winds: New = V - dt VU gV + dt dV
-  const double kE = kb(F_VE), kN = kb(F_VN), kT = kb(F_T);
   double VEb = kE + fa.sweep_adj(c, a, F_VE, i, -dt * VU * kE, dt * kE);
   double VNb = kN + fa.sweep_adj(c, a, F_VN, i, -dt * VU * kN, dt * kN);
   double VUb = -dt * gE * kE - dt * gN * kN;
@@ -771,7 +776,7 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
 
 // The limited slopes of cell i (interior: 4th-order form; cells 0 and
 // nAlts+1: 2nd-order form), as rusanov_slopes_cell forms them, with each
-// slope's limiter branch recorded for slopes_adjoint.
+// slope's limiter branch recorded for slopes_adjoint_window.
 __device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, int i, double beta) {
   const int nA = c.L.nAlts;
   const bool end = (i == 0 || i == nA + 1);
@@ -790,30 +795,44 @@ __device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, in
   }
 }
 
-// Adjoint of the limited slopes of cell i into the state adjoint, on the
-// branches slopes_with_branches recorded.
-__device__ inline void slopes_adjoint(const ColCtx& c, const ColAdj& a, int i, double beta) {
+// Adjoint of the limited slopes into the state adjoint, on the branches
+// slopes_with_branches recorded.  The slope of cell i is limiter_mc(u, d)
+// with u = cu (fa (v[i+1] - v[i]) - fb (v[i+2] - v[i-1])) and d = cd (fa
+// (v[i] - v[i-1]) - fb (v[i+1] - v[i-2])) (fa = 1, fb = 0 at the end
+// cells); its adjoint ob gives u the adjoint ub and d the adjoint dbv by
+// the branch, and those go to cells i-2..i+2.  One thread walks the slopes
+// of field f along cells j0-2..j1+2 and owns the state cells j0..j1
+// (within -1..nAlts+2): each slope is read once, its five shares are kept
+// in a window of partial sums, and a cell is written once it is complete
+// (no atomics).
+__device__ inline void slopes_adjoint_window(const ColCtx& c, const ColAdj& a, int f, int j0, int j1,
+                                             double beta) {
   const int nA = c.L.nAlts;
-  const bool end = (i == 0 || i == nA + 1);
-  // end cells: u = (v[i+1] - v[i]) cu, d = (v[i] - v[i-1]) cd; interior:
-  // the 4th-order differences with the mesh factors cu, cd
-  const double cu = end ? c.g(GC_IDF, i + 1) : c.g(GC_H2, i + 1);
-  const double cd = end ? c.g(GC_IDF, i) : c.g(GC_H2, i);
-  const double fa = end ? 1.0 : F1, fb = end ? 0.0 : F2;
-  const int ip2 = min(i + 2, nA + 2), im2 = max(i - 2, -1);
-  for (int f = 0; f < NSTENCIL; ++f) {
-    const double ob = a.db[f * (nA + 2) + i];
-    const int br = a.lc[f * (nA + 2) + i];
-    if (ob == 0.0 || br == 0) continue;
+  const double* __restrict__ dbp = a.db + f * (nA + 2);
+  const uint8_t* __restrict__ lcp = a.lc + f * (nA + 2);
+  double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0, w4 = 0.0;  // partial sums of cells i-2 .. i+2
+  for (int i = j0 - 2; i <= j1 + 2; ++i) {
+    const bool ok = (i >= 0 && i <= nA + 1);  // slopes exist at cells 0..nAlts+1
+    const int ic = min(max(i, 0), nA + 1);
+    const bool end = (ic == 0 || ic == nA + 1);
+    const double cu = end ? c.g(GC_IDF, ic + 1) : c.g(GC_H2, ic + 1);
+    const double cd = end ? c.g(GC_IDF, ic) : c.g(GC_H2, ic);
+    const double fa = end ? 1.0 : F1, fb = end ? 0.0 : F2;
+    const double ob = ok ? dbp[ic] : 0.0;
+    const int br = lcp[ic];
     const double ub = (br == 1) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
     const double dbv = (br == 2) ? beta * ob : (br == 3) ? 0.5 * ob : 0.0;
-    // one form for both kinds of cell (fa = 1, fb = 0 at the ends): the
-    // end cells add zeros to their clamped outer neighbours
-    a.add(f, ip2, -cu * fb * ub);
-    a.add(f, i + 1, cu * fa * ub - cd * fb * dbv);
-    a.add(f, i, -cu * fa * ub + cd * fa * dbv);
-    a.add(f, i - 1, cu * fb * ub - cd * fa * dbv);
-    a.add(f, im2, cd * fb * dbv);
+    w4 += -cu * fb * ub;                   // cell i+2
+    w3 += cu * fa * ub - cd * fb * dbv;    // cell i+1
+    w2 += -cu * fa * ub + cd * fa * dbv;   // cell i
+    w1 += cu * fb * ub - cd * fa * dbv;    // cell i-1
+    w0 += cd * fb * dbv;                   // cell i-2: complete
+    if (i - 2 >= j0) a.x(f, i - 2) += w0;
+    w0 = w1;
+    w1 = w2;
+    w2 = w3;
+    w3 = w4;
+    w4 = 0.0;
   }
 }
 
@@ -1122,44 +1141,61 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       for (int r = A.DB + tid; r < A.stride; r += NT) col[r] = 0.0;
     }
     __syncthreads();  // @phase 0
-    // scatter^T (advance_vertical.f90:163-217 and the heating line)
+    // scatter^T (advance_vertical.f90:163-217 and the heating line).  The
+    // cell's output adjoints are read into registers first: read between
+    // the shared-memory updates, each load would wait for the one before.
     for (int w = tid; w < nc * G; w += NT) {
       const int g = w / nc, cl = w - g * nc, i = g - 1;
       if (sfrozen[cl]) continue;
+      const bool ions = prm.use_ion_advection != 0;
+      const bool pc = in_pcells(i, nA);
+      const bool interior = (i >= 1 && i <= nA);
+      const double y_rho = B.rho[gidx(0, g, cl)];
+      const double y_ve = B.velocity[gidx(0, g, cl)];
+      const double y_vn = B.velocity[gidx(1, g, cl)];
+      const double y_vu = B.velocity[gidx(2, g, cl)];
+      const double ytemp = B.temperature[gidx(0, g, cl)];
+      const bool heat = b.heating && interior && B.heating_scale;
+      const double hq = heat ? b.heating[gidx(0, g, cl)] : 0.0;
+      const double yN = B.ndensity ? B.ndensity[gidx(0, g, cl)] : 0.0;
+      double y_w[NS], y_nd[NS], y_ln[NS], y_ion[NI];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        y_w[s] = B.vert_vel[gidx(s, g, cl)];
+        y_nd[s] = B.ndensity_s[gidx(s, g, cl)];
+        y_ln[s] = B.log_ns ? B.log_ns[gidx(s, g, cl)] : 0.0;
+      }
+      const double ye = ions ? B.idensity_s[gidx(NI, g, cl)] : 0.0;
+#pragma unroll
+      for (int s = 0; s < NI; ++s) y_ion[s] = (ions && (s < NADV || pc)) ? B.idensity_s[gidx(s, g, cl)] : 0.0;
       ColCtx c = ctx(cl);
       ColAdj a = adj(cl);
       const double tu = c.tu(i);
       const double LR4 = c.x(F_LRHO, i), T4 = c.x(F_T, i);
-      a.x(F_LRHO, i) += B.rho[gidx(0, g, cl)] * exp(LR4);
-      a.x(F_VE, i) += B.velocity[gidx(0, g, cl)];
-      a.x(F_VN, i) += B.velocity[gidx(1, g, cl)];
-      a.x(F_VU, i) += B.velocity[gidx(2, g, cl)];
-      const double ytemp = B.temperature[gidx(0, g, cl)];
+      a.x(F_LRHO, i) += y_rho * exp(LR4);
+      a.x(F_VE, i) += y_ve;
+      a.x(F_VN, i) += y_vn;
+      a.x(F_VU, i) += y_vu;
       a.x(F_T, i) += ytemp / tu;
       a.tub[i + 1] += -(ytemp * T4 / tu) / tu;
-      if (b.heating && i >= 1 && i <= nA && B.heating_scale)
-        atomicAdd(&a.mmb[2], ytemp * dt * b.heating[gidx(0, g, cl)]);
-      const double yN = B.ndensity ? B.ndensity[gidx(0, g, cl)] : 0.0;
+      if (heat) atomicAdd(&a.mmb[2], ytemp * dt * hq);
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        a.x(F_W + s, i) += B.vert_vel[gidx(s, g, cl)];
+        a.x(F_W + s, i) += y_w[s];
         const double L4 = c.x(F_LNS + s, i);
-        double v = (B.ndensity_s[gidx(s, g, cl)] + yN) * exp(L4);
-        if (B.log_ns) v += B.log_ns[gidx(s, g, cl)];
+        double v = (y_nd[s] + yN) * exp(L4);
+        if (B.log_ns) v += y_ln[s];
         a.x(F_LNS + s, i) += v;
       }
-      if (prm.use_ion_advection) {
+      if (ions) {
         const bool improved = prm.use_improved_ion_advection != 0;
-        const bool pc = in_pcells(i, nA);
-        const bool interior = (i >= 1 && i <= nA);
-        const double ye = B.idensity_s[gidx(NI, g, cl)];
 #pragma unroll
         for (int s = 0; s < NI; ++s) {
           if (!(s < NADV || pc)) continue;
           const double I4 = c.ion(s, i);
           const double v = improved ? I4 : exp(I4);
           const bool floored = improved && interior && v < 1;
-          const double yb = B.idensity_s[gidx(s, g, cl)] + ye;
+          const double yb = y_ion[s] + ye;
           a.ion(s, i) += floored ? 0.0 : (improved ? yb : yb * v);
         }
       }
@@ -1201,14 +1237,24 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         ColAdj a = adj(my_cl);
         eddy_bar += cell_adjoint_species(c, a, my_i, prm, dt, eddy, kbs, NT);
         cell_adjoint_rest(c, a, my_i, dt, ivup, kbs, NT);
-        // K = New - state: the state's own -K
+        // K = New - state: the state's own -K (K read into registers first:
+        // read between the shared atomics, each load would wait for the last)
+        double kv[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) a.add(f, my_i, -kbs[size_t(f) * NT]);
+        for (int f = 0; f < NF; ++f) kv[f] = kbs[size_t(f) * NT];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) a.add(f, my_i, -kv[f]);
       }
       __syncthreads();  // @phase 9
-      for (int j = tid; j < nc * (nA + 2); j += NT) {
-        const int cl = j / (nA + 2), i = j - cl * (nA + 2);
-        slopes_adjoint(ctx(cl), adj(cl), i, prm.beta_limiter);
+      {
+        // (column, field, run of cells) per thread
+        const int nseg = max(1, NT / (nc * NSTENCIL));
+        const int seg = (G + nseg - 1) / nseg;
+        for (int w = tid; w < nc * NSTENCIL * nseg; w += NT) {
+          const int sg = w % nseg, r = w / nseg, f = r % NSTENCIL, cl = r / NSTENCIL;
+          const int j0 = -1 + sg * seg, j1 = min(j0 + seg - 1, nA + 2);
+          if (j0 <= j1) slopes_adjoint_window(ctx(cl), adj(cl), f, j0, j1, prm.beta_limiter);
+        }
       }
       __syncthreads();  // @phase 10
       if (k > 0) {
@@ -1241,24 +1287,29 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
     for (int w = tid; w < nc * G; w += NT) {
       const int g = w / nc, cl = w - g * nc, i = g - 1;
       if (sfrozen[cl]) continue;
-      ColCtx c = ctx(cl);
-      ColAdj a = adj(cl);
-      // the step's inputs and the adjoint arrays do not overlap: restrict
-      // lets the loads of one cell be issued ahead of its stores
-      const double* __restrict__ in_nd = b.ndensity_s;
-      const double* __restrict__ in_ww = b.vert_vel;
-      const double* __restrict__ in_rho = b.rho;
-      const double* __restrict__ in_ion = b.idensity_s;
-      double* __restrict__ out_ion = B.idensity_s;
-      double nd[NS], ww[NS], ndb[NS], wwb[NS];
+      // every global value of the cell is read before its first global
+      // store (a store could alias a later load, which would then wait)
+      const bool ions = prm.use_ion_advection != 0;
+      const bool pc = in_pcells(i, nA);
+      double nd[NS], ww[NS], ndb[NS], wwb[NS], iv[NI];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        nd[s] = in_nd[gidx(s, g, cl)];
-        ww[s] = in_ww[gidx(s, g, cl)];
+        nd[s] = b.ndensity_s[gidx(s, g, cl)];
+        ww[s] = b.vert_vel[gidx(s, g, cl)];
+      }
+      const double temperature = b.temperature[gidx(0, g, cl)];
+      const double rho_in = b.rho[gidx(0, g, cl)];
+      const double ye = ions ? B.idensity_s[gidx(NI, g, cl)] : 0.0;
+#pragma unroll
+      for (int s = 0; s < NI; ++s)
+        iv[s] = !ions ? 0.0 : (s < NADV || pc) ? b.idensity_s[gidx(s, g, cl)] : B.idensity_s[gidx(s, g, cl)];
+      ColCtx c = ctx(cl);
+      ColAdj a = adj(cl);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
         ndb[s] = a.x(F_LNS + s, i) / nd[s];
         wwb[s] = a.x(F_W + s, i);
       }
-      const double temperature = b.temperature[gidx(0, g, cl)];
       const double tu = c.tu(i);
       double tb = a.x(F_T, i) * tu;
       double tub = a.tub[i + 1] + a.x(F_T, i) * temperature;
@@ -1307,21 +1358,19 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       B.velocity[gidx(0, g, cl)] = a.x(F_VE, i);
       B.velocity[gidx(1, g, cl)] = a.x(F_VN, i);
       B.velocity[gidx(2, g, cl)] = a.x(F_VU, i);
-      B.rho[gidx(0, g, cl)] = a.x(F_LRHO, i) / in_rho[gidx(0, g, cl)];
-      if (prm.use_ion_advection) {
+      B.rho[gidx(0, g, cl)] = a.x(F_LRHO, i) / rho_in;
+      if (ions) {
         const bool improved = prm.use_improved_ion_advection != 0;
-        const bool pc = in_pcells(i, nA);
-        const double ye = out_ion[gidx(NI, g, cl)];
 #pragma unroll
         for (int s = 0; s < NI; ++s) {
-          if (s < NADV || pc) {
-            const double v = in_ion[gidx(s, g, cl)];
-            out_ion[gidx(s, g, cl)] = improved ? a.ion(s, i) : a.ion(s, i) / v;
-          } else {
-            out_ion[gidx(s, g, cl)] += ye;  // unchanged by the step, summed into e-
-          }
+          // advected ions: the state value iv; the others: their own
+          // output adjoint iv, unchanged by the step, summed into e-
+          if (s < NADV || pc)
+            B.idensity_s[gidx(s, g, cl)] = improved ? a.ion(s, i) : a.ion(s, i) / iv[s];
+          else
+            B.idensity_s[gidx(s, g, cl)] = iv[s] + ye;
         }
-        out_ion[gidx(NI, g, cl)] = 0.0;
+        B.idensity_s[gidx(NI, g, cl)] = 0.0;
       }
     }
     if (tid < nc && !sfrozen[tid] && b.heating && B.heating_scale)
