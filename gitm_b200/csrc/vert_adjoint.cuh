@@ -785,13 +785,18 @@ __device__ inline void slopes_with_branches(const ColCtx& c, const ColAdj& a, in
   // both forms in one expression, as rusanov_slopes_cell
   const double fa = end ? 1.0 : F1, fb = end ? 0.0 : F2;
   const int ip2 = min(i + 2, nA + 2), im2 = max(i - 2, -1);
+  // state, slopes and branch bytes are disjoint regions (restrict: the
+  // loads of later fields may be issued ahead of earlier stores)
+  const double* __restrict__ xv = c.col + c.xo + 1;
+  double* __restrict__ sl = c.col + c.L.DL + i;
+  uint8_t* __restrict__ br = a.lc + i;
 #pragma unroll 3
   for (int f = 0; f < NSTENCIL; ++f) {
-    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    const double* v = xv + f * c.L.G;
     const double u = cu * (fa * (v[i + 1] - v[i]) - fb * (v[ip2] - v[i - 1]));
     const double d = cd * (fa * (v[i] - v[i - 1]) - fb * (v[i + 1] - v[im2]));
-    c.dl(f, i) = limiter_mc(u, d, beta);
-    a.lc[f * (nA + 2) + i] = uint8_t(limiter_mc_branch(u, d, beta));
+    sl[f * (nA + 2)] = limiter_mc(u, d, beta);
+    br[f * (nA + 2)] = uint8_t(limiter_mc_branch(u, d, beta));
   }
 }
 

@@ -602,12 +602,16 @@ __device__ __forceinline__ void rusanov_slopes_cell(ColCtx c, int i, double beta
   // are clamped into the column (finite values the zero factor removes)
   const double a = end ? 1.0 : F1, b = end ? 0.0 : F2;
   const int ip2 = min(i + 2, nA + 2), im2 = max(i - 2, -1);
+  // the state and slope regions of the column do not overlap: restrict
+  // lets the loads of later fields be issued ahead of earlier stores
+  const double* __restrict__ xv = c.col + c.xo + 1;
+  double* __restrict__ sl = c.col + c.L.DL + i;
 #pragma unroll 3
   for (int f = 0; f < NSTENCIL; ++f) {
-    const double* v = &c.col[c.xo + f * c.L.G + 1];
+    const double* v = xv + f * c.L.G;
     const double u = cu * (a * (v[i + 1] - v[i]) - b * (v[ip2] - v[i - 1]));
     const double d = cd * (a * (v[i] - v[i - 1]) - b * (v[i + 1] - v[im2]));
-    c.dl(f, i) = limiter_mc(u, d, beta);
+    sl[f * (nA + 2)] = limiter_mc(u, d, beta);
   }
 }
 
