@@ -140,6 +140,22 @@ def test_rollout_equals_stepwise_composition(cuda, every):
     run.close()
 
 
+def test_kept_stages_refused_when_they_do_not_fit(cuda):
+    """every = 0 with more steps than device memory holds stage states for
+    raises before the first step."""
+    from gitm_b200 import adjoint as AD
+    from gitm_b200 import vertical as V
+    m = synthetic.make_member(32, 50, seed=73)
+    ctx = V.VerticalContext(abi.default_params())
+    run = AD.StepRunner(ctx, m, 2.0, autotune=False)
+    free = torch.cuda.mem_get_info(cuda)[0]
+    n = int(free // run.stage_bytes_per_step()) + 1
+    with pytest.raises(V.GitmError, match="every > 0"):
+        AD.rollout(run, run.state(), n, 0)
+    run.close()
+    ctx.close()
+
+
 def test_rollout_matches_transcription_autograd(cuda):
     """A 20-step rollout: the adjoint's gradient against torch autograd
     through 20 steps of the transcription (the exact linearisation of the
