@@ -27,6 +27,7 @@ import os
 import re
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -99,7 +100,10 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.idx = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        # the raw samples go to GITM_CLOCKS_DIR when set (kept), else to a
+        # temporary directory
+        d = os.environ.get("GITM_CLOCKS_DIR") or tempfile.mkdtemp(prefix="gitm_clocks_")
+        self.path = os.path.join(d, f"clocks_rank{device_index}.csv")
 
     def start(self):
         try:
