@@ -26,6 +26,7 @@ import math
 import os
 import re
 import statistics
+import shutil
 import subprocess
 import tempfile
 import sys
@@ -102,7 +103,9 @@ class ClockSampler:
         self.proc = None
         # the raw samples go to GITM_CLOCKS_DIR when set (kept), else to a
         # temporary directory
-        d = os.environ.get("GITM_CLOCKS_DIR") or tempfile.mkdtemp(prefix="gitm_clocks_")
+        keep = os.environ.get("GITM_CLOCKS_DIR")
+        d = keep or tempfile.mkdtemp(prefix="gitm_clocks_")
+        self.tmp = None if keep else d
         self.path = os.path.join(d, f"clocks_rank{device_index}.csv")
 
     def start(self):
@@ -116,6 +119,13 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
+        try:
+            return self._read()
+        finally:
+            if self.tmp:
+                shutil.rmtree(self.tmp, ignore_errors=True)
+
+    def _read(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
