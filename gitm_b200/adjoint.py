@@ -159,7 +159,8 @@ class _Rollout(torch.autograd.Function):
         ckpts, stages = [], []
         if every == 0:
             need = n_steps * runner.stage_bytes_per_step()
-            free = torch.cuda.mem_get_info(runner.tensors["rho"].device)[0]
+            dev = runner.tensors["rho"].device
+            free = torch.cuda.mem_get_info(dev)[0] if dev.type == "cuda" else float("inf")
             if need > 0.9 * free:
                 raise V.GitmError(f"rollout with every = 0 keeps {need / 1e9:.1f} GB of stage states, "
                                   f"{free / 1e9:.1f} GB free: use checkpoints (every > 0)")
