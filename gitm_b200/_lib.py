@@ -31,6 +31,7 @@ SIGNATURES = {
     "gitm_vert_plan_autotune": (C.c_int, [_P, C.c_double, C.c_int, C.POINTER(abi.GitmLaunchConfig)]),
     "gitm_vert_plan_status": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_int]),
     "gitm_vert_plan_status_words": (_P, [_P]),
+    "gitm_vert_plan_wait": (C.c_int, [_P, _P, C.c_double]),
     "gitm_vert_plan_launch_count": (C.c_int, [_P, C.c_int]),
     "gitm_vert_advance_native": (C.c_int, [_P, C.POINTER(abi.GitmColumnBatch), C.c_int, C.c_double,
                                            C.c_int]),

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "vert_common.cuh"
@@ -47,9 +48,13 @@ struct GitmVertCtx {
   int64_t hz_status_n = 0;
   int64_t hz_blocks = 0;
   cudaStream_t hz_stream = nullptr;
+  // device address of the no-allocation entry point's file-scope scratch on
+  // this context's device, looked up when the context is created
+  double* noalloc_scratch = nullptr;
 };
 
 static int arena_reserve(GitmVertCtx* ctx, size_t bytes);
+static cudaError_t noalloc_scratch_address(double** out);
 struct GitmVertPlan;
 static void plan_free(GitmVertPlan* P);
 
@@ -332,6 +337,12 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
   if (adjoint_set_consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
   for (const StepInstance& si : kInstances)
     if (si.consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
+  // the scratch of gitm_vert_advance_native_noalloc on this device (a host-side
+  // name of a __device__ array is not its device address)
+  if (noalloc_scratch_address(&ctx->noalloc_scratch) != cudaSuccess || !ctx->noalloc_scratch) {
+    delete ctx;
+    return GITM_ERR_CUDA;
+  }
   for (int t : kThreadChoices)
     for (int io = 0; io < 2; ++io)
       for (int solver : {GITM_SOLVER_RUSANOV, GITM_SOLVER_AUSM})
@@ -615,7 +626,7 @@ static int launch_steps(GitmVertPlan* P, double dt, int n_steps, cudaStream_t st
   const void* fn = kernel_for(P->io, P->solver, P->cfg.threads);
   if (!fn) return set_err(ctx, GITM_ERR_ARG, "no kernel for %d threads", P->cfg.threads);
   const int grid = P->grid;
-  KParams kp;
+  KParams kp{};
   kp.members = P->d_members;
   kp.tiles = P->d_tiles;
   kp.n_tiles = int(P->tiles.size());
@@ -661,6 +672,36 @@ int gitm_vert_plan_status(GitmVertPlan* P, uint32_t* status_or, int64_t* n_bad, 
 }
 
 uint32_t* gitm_vert_plan_status_words(GitmVertPlan* P) { return P ? P->d_status : nullptr; }
+
+// Host watchdog (the reference has none; stop_gitm covers its failures): an
+// event recorded on `stream` is polled until it completes or timeout_s
+// passes.  Nothing on the device waits, so giving up leaves the context
+// usable: the work in flight still runs to completion.
+int gitm_vert_plan_wait(GitmVertPlan* P, void* stream, double timeout_s) {
+  if (!P) return GITM_ERR_ARG;
+  GitmVertCtx* ctx = P->ctx;
+  if (!(timeout_s >= 0.0)) return set_err(ctx, GITM_ERR_ARG, "timeout_s must be >= 0");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  cudaEvent_t ev = nullptr;
+  CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, static_cast<cudaStream_t>(stream));
+  const auto t0 = std::chrono::steady_clock::now();
+  while (e == cudaSuccess) {
+    e = cudaEventQuery(ev);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) break;
+    e = cudaSuccess;
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el >= timeout_s) {
+      cudaEventDestroy(ev);
+      return set_err(ctx, GITM_ERR_TIMEOUT, "the stream did not finish within %.3f s", timeout_s);
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  cudaEventDestroy(ev);
+  if (e != cudaSuccess) return set_err(ctx, GITM_ERR_CUDA, "waiting on the stream failed: %s", cudaGetErrorString(e));
+  return GITM_OK;
+}
 
 }  // extern "C"
 
@@ -878,7 +919,7 @@ extern "C" int gitm_vert_plan_advance_saving(GitmVertPlan* P, double dt, double*
   rc = adjoint_prepare(P);
   if (rc) return rc;
   if (P->adj_tiles.empty()) return GITM_OK;
-  KParams kp;
+  KParams kp{};
   std::memset(&kp, 0, sizeof kp);
   kp.members = P->d_members;
   kp.tiles = P->d_save_tiles;
@@ -1178,7 +1219,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     CUDA_TRY(ctx, cudaEventRecord(e_in, s_in));
     CUDA_TRY(ctx, cudaStreamWaitEvent(s_k, e_in, 0));
     const int spl = std::max(1, P->cfg.steps_per_launch);
-    KParams kp;
+    KParams kp{};
     std::memset(&kp, 0, sizeof kp);
     kp.members = P->d_members;
     kp.tiles = P->d_tiles + t0[j];
@@ -1529,9 +1570,8 @@ extern "C" int gitm_vert_advance_fortran(GitmVertCtx* ctx, const GitmFortranStat
 // ------------------------------------------------------------------ no-allocation entry point
 // gitm_vert_advance_native_noalloc: the step of one member without any device
 // allocation, for callers that cannot allocate device memory while they run:
-// a GITM host whose memory is held by its own pool (a caching allocator that
-// has reserved the GPU), code issued while a CUDA stream is being captured
-// (cudaMalloc cannot be captured), and per-step loops that must not pay the
+// a GITM host whose GPU memory is held by its own pool (a caching allocator
+// that has reserved the device), and per-step loops that must not pay the
 // device synchronisation an allocation implies.  Everything the step needs
 // beyond the caller's inputs and outputs -- the member descriptor, the tile
 // list, the grid coefficients and the RK accumulators of the persistent CTAs
@@ -1556,10 +1596,6 @@ static_assert(sizeof(Tile) == 2 * sizeof(double), "tile size");
 // or from different host threads) race on it: issue them in order.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-// Device address of g_noalloc_scratch, looked up once per device on the
-// first call made with that device current (a host-side name of a __device__
-// variable is not its device address).
-static double* g_noalloc_addr[64] = {};
 
 // Builds the member descriptor, the grid coefficients of the member's
 // shared altitude grid (the formulas of grid_coefs above) and the tile list
@@ -1638,6 +1674,15 @@ __global__ void noalloc_setup_kernel(GitmColumnBatch b, int nc, int n_tiles, dou
 
 }  // namespace
 
+// The device address of g_noalloc_scratch on the current device; called by
+// gitm_vert_create with the context's device current.
+static cudaError_t noalloc_scratch_address(double** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  *out = (e == cudaSuccess) ? static_cast<double*>(p) : nullptr;
+  return e;
+}
+
 extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColumnBatch* member,
                                                 double dt, int n_steps, uint32_t* status_words,
                                                 void* stream) {
@@ -1655,14 +1700,17 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   if (!(dt > 0.0)) return set_err(ctx, GITM_ERR_ARG, "dt must be > 0");
   if (n_steps < 0) return set_err(ctx, GITM_ERR_ARG, "n_steps < 0");
   if (b.n_cols == 0 || n_steps == 0) return GITM_OK;
-  if (ctx->device < 0 || ctx->device >= 64) return set_err(ctx, GITM_ERR_ARG, "device index out of range");
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
-  if (!g_noalloc_addr[ctx->device]) {
-    void* p = nullptr;
-    CUDA_TRY(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_addr[ctx->device] = static_cast<double*>(p);
-  }
-  double* base = g_noalloc_addr[ctx->device];
+  // the kernels read every pointer of the member on the device: host arrays
+  // are refused here (pointer queries enqueue no work and allocate nothing)
+  const void* ptrs[] = {b.ndensity_s, b.idensity_s, b.rho, b.temperature, b.velocity, b.vert_vel,
+                        b.log_ns, b.ndensity, b.gamma, b.mean_major_mass, b.temp_unit, b.cmax,
+                        b.ivel_up, b.eddy, b.cos_lat, b.sza, b.mlat, b.lbc, b.altitude, b.gravity,
+                        b.dalt_c, b.inv_r, b.heating, b.heating_scale, status_words};
+  for (const void* p : ptrs)
+    if (!is_device_ptr(p))
+      return set_err(ctx, GITM_ERR_ARG, "the no-allocation step takes device pointers only");
+  double* base = ctx->noalloc_scratch;
   const int nA = b.n_alts;
   int nc = std::min(kNoAllocThreads / nA, kNoAllocThreads / 32);
   while (nc > 1 && smem_bytes(nA, nc) > ctx->max_smem) --nc;
@@ -1674,7 +1722,7 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   CUDA_TRY(ctx, cudaMemsetAsync(status_words, 0, size_t(b.n_cols) * sizeof(uint32_t), st));
   noalloc_setup_kernel<<<1, 128, 0, st>>>(b, nc, n_tiles, base);
   CUDA_TRY(ctx, cudaGetLastError());
-  KParams kp;
+  KParams kp{};
   kp.members = reinterpret_cast<const DevMember*>(base);
   kp.tiles = reinterpret_cast<const Tile*>(base + kNoAllocDescDoubles + kNoAllocGridDoubles);
   kp.n_tiles = n_tiles;
@@ -1684,6 +1732,8 @@ extern "C" int gitm_vert_advance_native_noalloc(GitmVertCtx* ctx, const GitmColu
   kp.scratch = base + kNoAllocDescDoubles + kNoAllocGridDoubles + kNoAllocTileDoubles;
   kp.prm = ctx->params;
   void* args[] = {&kp};
+  // CTA x keeps its RK accumulators at scratch + x * NF * kNoAllocThreads:
+  // the grid never exceeds the kNoAllocSlots slots kNoAllocAccDoubles holds
   const int grid = std::min(n_tiles, kNoAllocSlots);
   CUDA_TRY(ctx, cudaLaunchKernel(kernel_for(0, GITM_SOLVER_RUSANOV, kNoAllocThreads), dim3(grid),
                                  dim3(kNoAllocThreads), args, smem, st));

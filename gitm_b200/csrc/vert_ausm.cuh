@@ -204,7 +204,7 @@ __device__ __forceinline__ void species_face_flux(double rl, double rr, double p
 // sound speed; the second forms the species fluxes and applies them.
 template <class Emit>
 __device__ __forceinline__ void ausm_cell(ColCtx c, int i, const GitmVertParams& prm, double dtk,
-                                          double eddy, double ivup, Emit&& emit) {
+                                          double eddy, double ivup, Emit&& emit, uint32_t* st = nullptr) {
   const int nA = c.L.nAlts;
   (void)nA;
   const double logk = c_k.log_kb;
@@ -349,7 +349,7 @@ __device__ __forceinline__ void ausm_cell(ColCtx c, int i, const GitmVertParams&
   if (prm.use_neutral_friction) {
     double glc[NS];
     grad_log_cons(c, i, glc);
-    friction_solve(dtk, nns, T, eddy, glc, wv);
+    friction_solve(dtk, nns, T, eddy, glc, wv, st);
   }
   // clamp and bulk vertical wind (:916-941)
   double NewVU = 0.0;

@@ -428,9 +428,15 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
 // solves (I + dt C) v = w in place and adds the eddy term -Eddy GradLogConS.
 // C_ij = 1e-2 k / (M_i D0_ij) n_j T^(1 - DiffExp_ij) (the NDensity factors of
 // the reference cancel); LU without pivoting, the matrix being strictly
-// diagonally dominant by rows.
+// diagonally dominant by rows for finite inputs.  ludcmp stops the run on a
+// row without an element of nonzero magnitude (ludcmp.f:9-17; NaN compares
+// false there, so a row of NaN counts): such a row sets GITM_ST_LU_SINGULAR
+// in *st (when st is given) and the solve goes on, its results non-finite.
+// A finite nonzero diagonal settles a row, so the scan of the whole row runs
+// only when the diagonal fails.
 __device__ __forceinline__ void friction_solve(double dt, const double (&ns)[NS], double T, double eddy,
-                                               const double (&glc)[NS], double (&wv)[NS]) {
+                                               const double (&glc)[NS], double (&wv)[NS],
+                                               uint32_t* st = nullptr) {
   const double lt = log(T);
   double pw[NS];
 #pragma unroll
@@ -447,6 +453,23 @@ __device__ __forceinline__ void friction_solve(double dt, const double (&ns)[NS]
       rs = rs + cij;
     }
     a[r][r] = 1.0 + dt * rs;
+  }
+  if (st) {
+    bool diag_ok = true;
+#pragma unroll
+    for (int r = 0; r < NS; ++r) diag_ok = diag_ok && (fabs(a[r][r]) > 0.0);
+    if (!diag_ok) {
+      bool singular = false;
+#pragma unroll
+      for (int r = 0; r < NS; ++r) {
+        double mx = 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+          if (fabs(a[r][q]) > mx) mx = fabs(a[r][q]);
+        singular = singular || !(mx > 0.0);
+      }
+      if (singular) atomicOr(st, GITM_ST_LU_SINGULAR);
+    }
   }
 #pragma unroll
   for (int p = 0; p < NS; ++p) {
@@ -495,10 +518,12 @@ constexpr double F2 = 0.0416667;  // Factor2, vertical_solver_rusanov.f90:740
 
 // advance_vertical_1stage (vertical_solver_rusanov.f90:387-686) at interior
 // cell i of the stage state in c, from the limited slopes in c's slope
-// buffer; emit(f, New - state) takes each field's increment.
+// buffer; emit(f, New - state) takes each field's increment.  st (may be
+// null) receives the column's GITM_ST_LU_SINGULAR bit.
 template <class Emit>
 __device__ __forceinline__ void rusanov_cell(ColCtx c, int i, const GitmVertParams& prm, double dt,
-                                             double eddy, double ivup, double inv_vert_tau, Emit&& emit) {
+                                             double eddy, double ivup, double inv_vert_tau, Emit&& emit,
+                                             uint32_t* st = nullptr) {
   const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1);
   const double idc = c.g(GC_IDC, i);
   const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
@@ -572,7 +597,7 @@ __device__ __forceinline__ void rusanov_cell(ColCtx c, int i, const GitmVertPara
     // GradLogConS (:506-543), LogConS = log(m_s) + LogNS - LogRho
     double glc[NS];
     grad_log_cons(c, i, glc);
-    friction_solve(dt, ns, T, eddy, glc, wv);
+    friction_solve(dt, ns, T, eddy, glc, wv, st);
   }
   // clamp and bulk vertical wind (:643-658)
   double vu = 0.0;
@@ -959,9 +984,9 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           };
           if constexpr (SOLVER == GITM_SOLVER_AUSM) {
             // advance_vertical_1stage_ausm with DtIn = Dt/2, Dt/2, Dt, Dt/2
-            ausm_cell(c, i, prm, (k == 2) ? dt : 0.5 * dt, eddy, ivup, emit);
+            ausm_cell(c, i, prm, (k == 2) ? dt : 0.5 * dt, eddy, ivup, emit, &sst[my_cl]);
           } else {
-            rusanov_cell(c, i, prm, dt, eddy, ivup, inv_vert_tau, emit);
+            rusanov_cell(c, i, prm, dt, eddy, ivup, inv_vert_tau, emit, &sst[my_cl]);
           }
         }
         // ghost cells and passive ions of the next buffer return to Orig

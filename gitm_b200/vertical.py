@@ -242,6 +242,16 @@ class Plan:
                self.ctx.handle, "plan_status")
         return st.value, nb.value
 
+    def wait(self, timeout_s: float, stream=None) -> bool:
+        """gitm_vert_plan_wait: True once the work issued on `stream` has
+        finished, False when timeout_s passed first (the work still runs)."""
+        s = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
+        rc = lib().gitm_vert_plan_wait(self.handle, C.c_void_p(s), float(timeout_s))
+        if rc == abi.ERR_TIMEOUT:
+            return False
+        _check(rc, self.ctx.handle, "plan_wait")
+        return True
+
     def check(self, clear: bool = True):
         st, nb = self.status(clear)
         if st:

@@ -253,6 +253,12 @@ int gitm_vert_plan_status(GitmVertPlan* plan, uint32_t* status_or,
                           int64_t* n_bad, int clear);
 /* Per-column status words, device array in member order (n_cols total). */
 uint32_t* gitm_vert_plan_status_words(GitmVertPlan* plan);
+/* Host watchdog, no counterpart in the reference: waits until the work
+ * issued on `stream` so far has finished, polling an event, and returns
+ * GITM_ERR_TIMEOUT when timeout_s passes first.  The work in flight still
+ * completes; the context stays usable.  timeout_s = 0 only asks whether the
+ * stream is idle. */
+int gitm_vert_plan_wait(GitmVertPlan* plan, void* stream, double timeout_s);
 /* Number of kernel launches one gitm_vert_plan_advance(.., n_steps, ..) issues. */
 int gitm_vert_plan_launch_count(const GitmVertPlan* plan, int n_steps);
 
@@ -272,17 +278,16 @@ int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnBatch* membe
 /* No counterpart in the reference.  n_steps RK4 steps of one member, like
  * the plan API, but allocating no device memory: for callers that cannot
  * allocate while they run -- a host whose GPU memory is held by its own pool,
- * code issued during CUDA stream capture (cudaMalloc cannot be captured),
  * and per-step loops that must not pay an allocation's device
- * synchronisation.  Device pointers; asynchronous on `stream`.
+ * synchronisation.  Device pointers only (host arrays are refused with
+ * GITM_ERR_ARG); asynchronous on `stream`.
  *   - The member descriptor, tile list, grid coefficients and RK
  *     accumulators live in one file-scope device array of 12.3 MiB that every
- *     GPU loading the library holds until the process exits.
+ *     GPU loading the library holds until the process exits;
+ *     gitm_vert_create looks up its device address.
  *   - Limits: n_cols <= 262144 and one altitude grid per member
  *     (grid_per_column = 0); larger or per-column-grid members are rejected
  *     with GITM_ERR_ARG.
- *   - The first call on a device looks up the array's device address; make
- *     that first call before any stream capture.
  *   - Every call reuses the array, so calls that overlap on the GPU race:
  *     issue them in order (one stream, or synchronise between streams).
  *   - status_words (device, n_cols words) are zeroed and then receive each

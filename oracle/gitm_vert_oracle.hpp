@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -358,8 +359,14 @@ void neutral_friction(double DtIn, R* oVel, const R* EddyCoef, const R* NDensity
     }
     int iPivot[7];
     R Parity;
-    if (!ludcmp(Matrix, nSpecies, iPivot, Parity)) status |= GITM_ST_LU_SINGULAR;
-    lubksb(Matrix, nSpecies, iPivot, Vel);
+    if (ludcmp(Matrix, nSpecies, iPivot, Parity)) {
+      lubksb(Matrix, nSpecies, iPivot, Vel);
+    } else {
+      // stop_gitm('singular matrix in ludcmp') ends the reference's run here;
+      // the column has no defined result, so its velocities become NaN
+      status |= GITM_ST_LU_SINGULAR;
+      for (int s = 1; s <= nSpecies; ++s) Vel[s] = std::numeric_limits<double>::quiet_NaN();
+    }
     for (int s = 1; s <= nSpecies; ++s) oVel[I2(iAlt, s)] = Vel[s] + EddyContribution[s];
   }
 }

@@ -1,26 +1,32 @@
 """The Fortran-layout drop-in (gitm_vert_advance_fortran) on ModGITM-shaped
-arrays in Fortran order, against the native path on the same columns."""
+arrays in Fortran order, against the oracle on the same columns.
+
+The blocks are 9 x 9 columns (GITM's default grid, Config.pl -g=9,9,50,4);
+the largest case is GITM's default run of 2 x 2 blocks = 324 columns at
+nAlts = 50, one step of dt = 2 s."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
 from gitm_b200 import abi, synthetic
+from tests.parity import assert_state_close
 
 pytestmark = pytest.mark.gpu
 
-NLON, NLAT, NALT, NBLK = 9, 9, 30, 2
+NLON, NLAT = 9, 9
 
 
-def fortran_arrays(m):
+def fortran_arrays(m, n_blk):
     """ModGITM arrays (Fortran order, halo'd) holding member m's columns,
     column c = (iBlock-1)*81 + (iLat-1)*9 + (iLon-1)."""
-    G = NALT + 4
+    n_alt = m.n_alts
+    G = n_alt + 4
     H = (NLON + 4, NLAT + 4, G)
     rng = np.random.default_rng(1)
 
     def halo(*extra):
-        return np.asfortranarray(rng.normal(size=H + extra + (NBLK,)))  # junk in halos
+        return np.asfortranarray(rng.normal(size=H + extra + (n_blk,)))  # junk in halos
 
     f = {
         "ndensity_s": halo(11), "idensity_s": halo(10), "rho": halo(), "temperature": halo(),
@@ -28,14 +34,14 @@ def fortran_arrays(m):
         "ndensity": halo(), "species_density": halo(20), "species_density_old": halo(20),
         "gamma": halo(), "altitude": halo(), "gravity": halo(), "dalt": halo(), "inv_r": halo(),
         "mlatitude": halo(),
-        "mean_major_mass": np.asfortranarray(rng.normal(size=H + (NBLK,))),  # per block slices
-        "temp_unit": np.asfortranarray(rng.normal(size=H + (NBLK,))),
-        "cmax": np.asfortranarray(rng.normal(size=(NLON + 2, NLAT + 2, NALT + 2, 3, NBLK))),
-        "kappa_eddy": np.asfortranarray(rng.normal(size=(NLON, NLAT, G, NBLK))),
-        "cos_latitude": np.asfortranarray(rng.normal(size=(NLAT + 4, NBLK))),
-        "sza": np.asfortranarray(rng.normal(size=(NLON, NLAT, NBLK))),
+        "mean_major_mass": np.asfortranarray(rng.normal(size=H + (n_blk,))),  # per block slices
+        "temp_unit": np.asfortranarray(rng.normal(size=H + (n_blk,))),
+        "cmax": np.asfortranarray(rng.normal(size=(NLON + 2, NLAT + 2, n_alt + 2, 3, n_blk))),
+        "kappa_eddy": np.asfortranarray(rng.normal(size=(NLON, NLAT, G, n_blk))),
+        "cos_latitude": np.asfortranarray(rng.normal(size=(NLAT + 4, n_blk))),
+        "sza": np.asfortranarray(rng.normal(size=(NLON, NLAT, n_blk))),
     }
-    for b in range(NBLK):
+    for b in range(n_blk):
         for j in range(NLAT):
             for i in range(NLON):
                 c = b * 81 + j * 9 + i
@@ -56,7 +62,7 @@ def fortran_arrays(m):
                 f["gravity"][li, lj, :, b] = m.gravity
                 f["dalt"][li, lj, :, b] = m.dalt_c
                 f["inv_r"][li, lj, :, b] = m.inv_r
-                f["mlatitude"][li, lj, NALT + 1, b] = m.mlat[c]
+                f["mlatitude"][li, lj, n_alt + 1, b] = m.mlat[c]
                 f["sza"][i, j, b] = m.sza[c]
                 f["cos_latitude"][lj, b] = m.cos_lat[c]
     return f
@@ -90,9 +96,9 @@ def descriptor(ptr, strides_elems, name, block_slice=None):
     return fa
 
 
-def state_struct(arrays, getptr):
+def state_struct(n_alts, n_blk, getptr):
     st = abi.GitmFortranState()
-    st.n_lons, st.n_lats, st.n_alts, st.n_blocks = NLON, NLAT, NALT, NBLK
+    st.n_lons, st.n_lats, st.n_alts, st.n_blocks = NLON, NLAT, n_alts, n_blk
     for name in abi.FORTRAN_ARRAYS:
         ptr, strides = getptr(name)
         setattr(st, name, descriptor(ptr, strides, name))
@@ -100,34 +106,31 @@ def state_struct(arrays, getptr):
 
 
 @pytest.mark.parametrize("on_device", [0, 1])
-def test_fortran_layout_matches_native(on_device):
+@pytest.mark.parametrize("n_blk,n_alt", [(2, 30), (4, 50)], ids=["2blocks_nalts30", "4blocks_nalts50"])
+def test_fortran_layout_matches_oracle(oracle_lib, on_device, n_blk, n_alt):
     import torch
     from gitm_b200 import _lib
     from gitm_b200 import vertical as V
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     p = abi.default_params(compute_coefficients=0)
-    m = synthetic.make_member(NLON * NLAT * NBLK, NALT, seed=41)
+    m = synthetic.make_member(NLON * NLAT * n_blk, n_alt, seed=41)
     # CosLatitude(iLat, iBlock) is one value per latitude row
-    for b in range(NBLK):
+    for b in range(n_blk):
         for j in range(NLAT):
             row = slice(b * 81 + j * 9, b * 81 + j * 9 + 9)
             m.cos_lat[row] = m.cos_lat[b * 81 + j * 9]
-    f = fortran_arrays(m)
+    f = fortran_arrays(m, n_blk)
     ns_in = f["ndensity_s"].copy()
-    # native reference on the same columns, through the entry point the
-    # Fortran form calls (device arrays: gitm_vert_advance_native; host
-    # arrays: gitm_vert_advance_native_host), so that the same kernel runs
+    # the oracle on the same columns (native layout, host memory)
+    r = m.copy()
+    r.log_ns = np.zeros_like(m.ndensity_s)
+    r.ndensity = np.zeros_like(m.rho)
+    st_ref = oracle_lib.advance(r, p, 2.0, 1)
+    assert (st_ref == 0).all()
+    ref = dict(r.arrays())
     ctx = V.VerticalContext(p)
-    if on_device:
-        dm = V.device_member(m)
-        V.advance_vertical_all(ctx, [dm], 2.0)
-        ref = dm.to_numpy()
-    else:
-        h = m.copy()
-        V.advance_vertical_all_host(ctx, [h], 2.0)
-        ref = dict(h.arrays())
-    for blk in range(1, NBLK + 1):
+    for blk in range(1, n_blk + 1):
         # MeanMajorMass / TempUnit hold one block (calc_rates(iBlock)): give
         # the descriptor this block's slice through a zero block stride
         if on_device:
@@ -150,30 +153,41 @@ def test_fortran_layout_matches_native(on_device):
                     ptr += (blk - 1) * strides[3] * 8
                     strides[3] = 0
                 return ptr, strides
-        st = state_struct(f, getptr)
+        st = state_struct(n_alt, n_blk, getptr)
         rc = _lib.lib().gitm_vert_advance_fortran(ctx.handle, C.byref(st), blk, blk, 2.0, on_device)
         assert rc == abi.OK, ctx.last_error()
         if on_device:
             torch.cuda.synchronize()
             for k in f:
                 f[k] = np.asfortranarray(tens[k].cpu().numpy())
-    G = NALT + 4
-    for b in range(NBLK):
+    ctx.close()
+    # gather the Fortran arrays back into the native layout and compare
+    n = NLON * NLAT * n_blk
+    G = n_alt + 4
+    got = {"ndensity_s": np.zeros((6, G, n)), "idensity_s": np.zeros((10, G, n)), "rho": np.zeros((1, G, n)),
+           "temperature": np.zeros((1, G, n)), "velocity": np.zeros((3, G, n)), "vert_vel": np.zeros((6, G, n)),
+           "log_ns": np.zeros((6, G, n)), "ndensity": np.zeros((1, G, n))}
+    sd_new, sd_old = np.zeros((20, G, n)), np.zeros((20, G, n))
+    for b in range(n_blk):
         for j in range(NLAT):
             for i in range(NLON):
                 c = b * 81 + j * 9 + i
                 li, lj = i + 2, j + 2
-                np.testing.assert_array_equal(f["ndensity_s"][li, lj, :, :6, b], ref["ndensity_s"][:, :, c].T)
-                np.testing.assert_array_equal(f["idensity_s"][li, lj, :, :, b], ref["idensity_s"][:, :, c].T)
-                np.testing.assert_array_equal(f["rho"][li, lj, :, b], ref["rho"][0, :, c])
-                np.testing.assert_array_equal(f["temperature"][li, lj, :, b], ref["temperature"][0, :, c])
-                np.testing.assert_array_equal(f["velocity"][li, lj, :, :, b], ref["velocity"][:, :, c].T)
-                np.testing.assert_array_equal(f["vertical_velocity"][li, lj, :, :, b], ref["vert_vel"][:, :, c].T)
-                np.testing.assert_array_equal(f["log_ns"][li, lj, :, :, b], ref["log_ns"][:, :, c].T)
-                np.testing.assert_array_equal(f["ndensity"][li, lj, :, b], ref["ndensity"][0, :, c])
-                # SpeciesDensityOld = state before, SpeciesDensity = after (advance_vertical.f90:152-155,214-217)
+                got["ndensity_s"][:, :, c] = f["ndensity_s"][li, lj, :, :6, b].T
+                got["idensity_s"][:, :, c] = f["idensity_s"][li, lj, :, :, b].T
+                got["rho"][0, :, c] = f["rho"][li, lj, :, b]
+                got["temperature"][0, :, c] = f["temperature"][li, lj, :, b]
+                got["velocity"][:, :, c] = f["velocity"][li, lj, :, :, b].T
+                got["vert_vel"][:, :, c] = f["vertical_velocity"][li, lj, :, :, b].T
+                got["log_ns"][:, :, c] = f["log_ns"][li, lj, :, :, b].T
+                got["ndensity"][0, :, c] = f["ndensity"][li, lj, :, b]
+                sd_new[:, :, c] = f["species_density"][li, lj, :, :, b].T
+                sd_old[:, :, c] = f["species_density_old"][li, lj, :, :, b].T
+                # SpeciesDensityOld = state before (advance_vertical.f90:152-155)
                 np.testing.assert_array_equal(f["species_density_old"][li, lj, :, :6, b], ns_in[li, lj, :, :6, b])
-                np.testing.assert_array_equal(f["species_density"][li, lj, :, :6, b], ref["ndensity_s"][:, :, c].T)
-                np.testing.assert_array_equal(f["species_density"][li, lj, :, 11:20, b], ref["idensity_s"][:9, :, c].T)
+    assert_state_close(got, ref, tuple(got))
+    # SpeciesDensity = NDensityS and IDensityS after the step (advance_vertical.f90:214-217)
+    np.testing.assert_array_equal(sd_new[:6], got["ndensity_s"])
+    np.testing.assert_array_equal(sd_new[11:20], got["idensity_s"][:9])
     # halo cells are untouched
     np.testing.assert_array_equal(f["ndensity_s"][0, :, :, :, :], ns_in[0, :, :, :, :])

@@ -94,19 +94,18 @@ def test_eddy_producer(torch_cuda, oracle_lib, solver, n_steps, spl):
     assert np.abs(out["eddy"] - m.eddy).max() > 0.0
 
 
-def test_eddy_producer_host_path(torch_cuda):
+def test_eddy_producer_host_path(torch_cuda, oracle_lib):
     """The host-pointer form copies the produced coefficient back."""
     from gitm_b200 import vertical as V
     p = abi.default_params(compute_eddy=1)
     m = synthetic.make_member(700, 50, seed=36)
-    # the launch shape of the host-pointer form: 128 threads, one step per launch
-    dev_out, _ = gpu_advance(m, p, 2.0, n_steps=2, config=dict(threads=128, steps_per_launch=1))
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0, n_steps=2)
     h = m.copy()
     ctx = V.VerticalContext(p)
     V.advance_vertical_all_host(ctx, [h], 2.0, n_steps=2)
-    for k in synthetic.Member.STATE + ("eddy",):
-        np.testing.assert_array_equal(getattr(h, k), dev_out[k], err_msg=k)
     ctx.close()
+    assert (st_ref == 0).all()
+    assert_state_close(dict(h.arrays()), ref, synthetic.Member.STATE + ("eddy",), rtol=1e-9)
 
 
 def test_eddy_producer_refused_by_adjoint(torch_cuda):
@@ -208,18 +207,53 @@ def test_one_shot_raises_gitmstop(torch_cuda):
         V.advance_vertical_all(ctx, [V.device_member(m)], 2.0)
 
 
-def test_host_pointer_path_matches_device(torch_cuda, oracle_lib):
+def test_host_pointer_path_matches_oracle(torch_cuda, oracle_lib):
+    """gitm_vert_advance_native_host (host arrays, chunked copies overlapped
+    with the steps) against the oracle, and bit for bit against the device
+    form with the launch shape the host form uses (128 threads, one step per
+    launch: each launch shape is compiled on its own and may round
+    differently)."""
     from gitm_b200 import vertical as V
     p = abi.default_params()
     m = synthetic.make_member(5000, 50, seed=28)
-    # the host-pointer form runs the 128-thread kernel one step per launch;
-    # each launch shape is compiled on its own and may round differently
-    dev_out, _ = gpu_advance(m, p, 2.0, config=dict(threads=128, steps_per_launch=1))
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0)
     h = m.copy()
     ctx = V.VerticalContext(p)
     V.advance_vertical_all_host(ctx, [h], 2.0)
+    ctx.close()
+    assert (st_ref == 0).all()
+    assert_state_close(dict(h.arrays()), ref, STATE)
+    dev_out, _ = gpu_advance(m, p, 2.0, config=dict(threads=128, steps_per_launch=1))
     for k in STATE:
         np.testing.assert_array_equal(getattr(h, k), dev_out[k], err_msg=k)
+
+
+def test_globe5deg_100_steps_each_against_the_oracle(torch_cuda, oracle_lib):
+    """The 5 deg globe (36 x 72 = 2,592 columns, GITM's 4 x 8 blocks of 9 x 9),
+    nAlts = 50, 100 RK4 steps of dt = 2 s through the plain per-call drop-in
+    (gitm_vert_advance_native, one call per step).  After every step the GPU
+    result is compared with one oracle step taken from the GPU's own previous
+    state, at the per-step tolerance of 1e-10, so rounding differences do not
+    accumulate across the comparison."""
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.globe_member(5.0, 5.0, n_alts=50, seed=1)
+    assert m.n_cols == 2592
+    ctx = V.VerticalContext(p)
+    dm = V.device_member(m)
+    cur = m.copy()
+    worst = 0.0
+    for step in range(100):
+        V.advance_vertical_all(ctx, [dm], 2.0)
+        out = dm.to_numpy()
+        ref, st_ref = ref_advance(oracle_lib, cur, p, 2.0)
+        assert (st_ref == 0).all(), f"step {step}: oracle status"
+        rep = assert_state_close(out, ref, STATE)
+        worst = max(worst, max(rep.values()))
+        for k in synthetic.Member.STATE + synthetic.Member.COEFFS:
+            setattr(cur, k, out[k].copy())
+    ctx.close()
+    print(f"100 steps of 2592 columns: worst per-step normwise rel err {worst:.3e}")
 
 
 def test_modvertical_form(torch_cuda, oracle_lib):
