@@ -251,21 +251,37 @@ static bool acc_global(int threads) {
 struct StepInstance {
   int io, threads, solver;
   bool save;
+  int na;  // 0: any nAlts; > 0: members of exactly this nAlts
   const void* (*fn)();
   cudaError_t (*consts)(const Consts&);
 };
 static const StepInstance kInstances[] = {
-#define GV_TABLE_ENTRY(id, IO, NT, MINB, ACC, SOLVER, SAVE) {IO, NT, SOLVER, SAVE, step_kernel_##id, step_consts_##id},
+#define GV_TABLE_ENTRY(id, IO, NT, MINB, ACC, SOLVER, SAVE, NA) \
+  {IO, NT, SOLVER, SAVE, NA, step_kernel_##id, step_consts_##id},
     GV_STEP_INSTANCES(GV_TABLE_ENTRY)
 #undef GV_TABLE_ENTRY
 };
 
 // The step kernel for an array form (0 GITM arrays, 1 ModVertical), solver
-// and CTA size, or nullptr when that shape is not built.
-static const void* kernel_for(int io, int solver, int threads) {
-  for (const StepInstance& k : kInstances)
-    if (!k.save && k.io == io && k.solver == solver && k.threads == threads) return k.fn();
-  return nullptr;
+// and CTA size, or nullptr when that shape is not built.  nalts > 0 (every
+// member has that nAlts) prefers the instance compiled for it.
+static const void* kernel_for(int io, int solver, int threads, int nalts = 0, bool save = false) {
+  const StepInstance* any = nullptr;
+  for (const StepInstance& k : kInstances) {
+    if (k.save != save || k.io != io || k.solver != solver || k.threads != threads) continue;
+    if (nalts > 0 && k.na == nalts) return k.fn();
+    if (k.na == 0 && !any) any = &k;
+  }
+  return any ? any->fn() : nullptr;
+}
+
+// The nAlts every member of a plan shares, or 0 when they differ.
+static int plan_nalts(const GitmVertPlan* P) {
+  if (P->host_members.empty()) return 0;
+  const int na = P->host_members[0].n_alts;
+  for (const GitmColumnBatch& b : P->host_members)
+    if (b.n_alts != na) return 0;
+  return na;
 }
 
 // ------------------------------------------------------------------ API
@@ -343,11 +359,8 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
     delete ctx;
     return GITM_ERR_CUDA;
   }
-  for (int t : kThreadChoices)
-    for (int io = 0; io < 2; ++io)
-      for (int solver : {GITM_SOLVER_RUSANOV, GITM_SOLVER_AUSM})
-        if (const void* fn = kernel_for(io, solver, t))
-          cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem));
+  for (const StepInstance& si : kInstances)
+    cudaFuncSetAttribute(si.fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem));
   *out = ctx;
   return GITM_OK;
 }
@@ -421,7 +434,7 @@ static int build_tiles(GitmVertPlan* P) {
   int grid = int(P->tiles.size());
   int per_sm = P->cfg.ctas_per_sm;
   if (acc_global(T) && per_sm <= 0) {
-    const void* fn = kernel_for(P->io, P->solver, T);
+    const void* fn = kernel_for(P->io, P->solver, T, plan_nalts(P));
     CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->smem));
     per_sm = std::max(per_sm, 1);
   }
@@ -623,7 +636,7 @@ static int launch_steps(GitmVertPlan* P, double dt, int n_steps, cudaStream_t st
   if (ctx->params.solver != P->solver)
     return set_err(ctx, GITM_ERR_ARG, "plan was built for solver %d, context now selects %d", P->solver,
                    ctx->params.solver);
-  const void* fn = kernel_for(P->io, P->solver, P->cfg.threads);
+  const void* fn = kernel_for(P->io, P->solver, P->cfg.threads, plan_nalts(P));
   if (!fn) return set_err(ctx, GITM_ERR_ARG, "no kernel for %d threads", P->cfg.threads);
   const int grid = P->grid;
   KParams kp{};
@@ -874,7 +887,8 @@ static int adjoint_prepare(GitmVertPlan* P) {
   }
   CUDA_TRY(ctx, cudaMalloc(&P->d_bars, std::max(1, P->n_members) * sizeof(GitmColumnAdjoint)));
   // the saving step kernel: its own tiles, the forward layout
-  const void* sfn = saving_kernel_fn();
+  const void* sfn = kernel_for(0, GITM_SOLVER_RUSANOV, SAVE_THREADS, plan_nalts(P), true);
+  if (!sfn) return set_err(ctx, GITM_ERR_ARG, "the saving step kernel is not built");
   CUDA_TRY(ctx, cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem)));
   int sper = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sper, sfn, TS, P->save_smem));
@@ -933,7 +947,7 @@ extern "C" int gitm_vert_plan_advance_saving(GitmVertPlan* P, double dt, double*
   kp.save_ncols = P->n_cols_total;
   kp.save_per = P->adj_per_max;
   void* args[] = {&kp};
-  CUDA_TRY(ctx, cudaLaunchKernel(saving_kernel_fn(), dim3(P->save_grid), dim3(SAVE_THREADS), args, P->save_smem,
+  CUDA_TRY(ctx, cudaLaunchKernel(kernel_for(0, GITM_SOLVER_RUSANOV, SAVE_THREADS, plan_nalts(P), true), dim3(P->save_grid), dim3(SAVE_THREADS), args, P->save_smem,
                                  static_cast<cudaStream_t>(stream)));
   return GITM_OK;
 }
@@ -1179,7 +1193,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
   for (int t = int(P->tiles.size()) - 1; t >= 0; --t) t0[P->tiles[t].member] = t;
   for (int j = int(chunks.size()) - 1; j >= 0; --j)
     if (t0[j] > t0[j + 1]) t0[j] = t0[j + 1];
-  const void* fn = kernel_for(0, P->solver, P->cfg.threads);
+  const void* fn = kernel_for(0, P->solver, P->cfg.threads, plan_nalts(P));
   // one stream per role: copies in (streams[0]), steps (streams[1]), copies
   // out (streams[2]); a chunk's step waits for its copies in and its copies
   // out wait for its step, so each copy engine streams without waiting for

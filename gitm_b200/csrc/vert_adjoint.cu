@@ -17,12 +17,6 @@ namespace gv {
 
 const void* adjoint_kernel_fn() { return (const void*)vert_adjoint_kernel<ADJ_THREADS>; }
 
-// The step kernel that also saves the stage states for the adjoint (GITM
-// arrays, Rusanov, 128 threads, accumulator in per-CTA scratch), built in a
-// translation unit of its own like the other step kernels.
-static_assert(SAVE_THREADS == 128, "the saving step kernel is built for 128 threads");
-const void* saving_kernel_fn() { return step_kernel_rus0_t128_save(); }
-
 cudaError_t adjoint_set_consts(const Consts& k) { return cudaMemcpyToSymbol(c_k, &k, sizeof k); }
 
 }  // namespace gv

@@ -57,7 +57,6 @@ constexpr int SAVE_THREADS = 128;
 
 // Defined in vert_adjoint.cu (the kernel's own translation unit).
 const void* adjoint_kernel_fn();
-const void* saving_kernel_fn();
 cudaError_t adjoint_set_consts(const Consts& k);
 __host__ __device__ inline int adj_state_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
 

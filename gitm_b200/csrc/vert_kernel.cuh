@@ -266,12 +266,11 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
       }
       const double r0 = lane_seq_sum(m0, NS), r1 = lane_seq_sum(m1, NS);
       const double v0 = lane_seq_sum(t0, NS), v1 = lane_seq_sum(t1, NS);
-      if (s == 0) {
-        x(F_LRHO, 0) = log(r0);
-        x(F_VU, 0) = v0 / r0;
-      } else if (s == 1) {
-        x(F_LRHO, -1) = log(r1);
-        x(F_VU, -1) = v1 / r1;
+      // lane 0 takes cell 0, lane 1 cell -1: one log and one division for both
+      if (s < 2) {
+        const double r = s ? r1 : r0;
+        x(F_LRHO, -s) = log(r);
+        x(F_VU, -s) = (s ? v1 : v0) / r;
       }
     }
     // lines 364-376
@@ -327,7 +326,8 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
       tp += c.dAF(i) * (improved ? v : exp(v));
     }
     for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
-    const bool hold = (tp / 1e16 < prm.min_tec) && (sc[SC_PLASMA] != 0.0);
+    // TEC / 1e16 < MinTEC (1e16 is exact in binary64)
+    const bool hold = (tp < prm.min_tec * 1e16) && (sc[SC_PLASMA] != 0.0);
     const double* bu = sc + SC_BCC + 10;  // upper mesh coefficients, nA+1 then nA+2
     // check_for_negative_densities (lines 608-649) can only act when a value
     // in nAlts-5 .. nAlts+2 is negative
@@ -396,11 +396,12 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
         double dn = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
         const double lim = -(0.001 * n[0] / sc[SC_DAF + 3]);
         if (dn > lim) dn = lim;
-        const double v = exp(n[1] + dn * sc[SC_DAF + 4]);
-        c.ion(s, nA + 1) = v;
-        // cell nAlts+2: logs of its own ghost and of the value just set
+        const double y = n[1] + dn * sc[SC_DAF + 4];
+        c.ion(s, nA + 1) = exp(y);
+        // cell nAlts+2: the log of its own ghost, and y for the log of the
+        // value just set (log(exp(y)) in the reference, y to rounding)
         const double g0 = log(c.ion(s, nA + 2));
-        n1 = log(v);
+        n1 = y;
         const double* D = bu + 5;
         double dn2 = D[0] * n1 + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
         const double lim2 = -(0.001 * g0 / sc[SC_DAF + 3]);
@@ -417,8 +418,7 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
         m2 = c_k.mass[s] * exp(x(F_LNS + s, nA + 2));
       }
       const double r1 = lane_seq_sum(m1, NS), r2 = lane_seq_sum(m2, NS);
-      if (s == 0) x(F_LRHO, nA + 1) = log(r1);
-      if (s == 1) x(F_LRHO, nA + 2) = log(r2);
+      if (s < 2) x(F_LRHO, nA + 1 + s) = log(s ? r2 : r1);
     }
   }
   __syncwarp();
@@ -669,7 +669,10 @@ struct KParams {
 // ACC_GLOBAL: the RK accumulator of each item lives in a per-CTA slot of
 // kp.scratch (coalesced, L2-resident under a persistent grid) instead of
 // registers, which lets small CTAs share an SM.
-template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER, bool SAVE = false>
+// NA > 0: every member has exactly NA altitudes (the host checks), so the
+// shared-memory layout, the item mapping and the loop bounds are
+// compile-time constants; NA = 0 reads nAlts from the member.
+template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER, bool SAVE = false, int NA = 0>
 __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
@@ -683,7 +686,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
   for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
     const Tile tile = kp.tiles[tix];
     const DevMember& M = kp.members[tile.member];
-    const int nA = M.b.n_alts;
+    const int nA = (NA > 0) ? NA : M.b.n_alts;
     const int nc = tile.nc;
     const Layout L = make_layout(nA, SOLVER);
     const int G = L.G;
