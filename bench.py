@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--plain-steps", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--sustained", type=float, default=2.0,
+                    help="seconds of device time of the sustained leg (0 = skip)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the AUSM, adjoint and ensemble legs of the default run")
+    ap.add_argument("--extra-fd", type=int, default=4,
+                    help="finite-difference directions of the adjoint leg of the default run")
     ap.add_argument("--solver", default="rusanov", choices=["rusanov", "ausm"])
     ap.add_argument("--adjoint", action="store_true",
                     help="measure the adjoint rollout (2.5 deg globe, 60 steps, checkpoint every 10)")
@@ -92,25 +98,66 @@ def dist_env():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    """SM clock, power and clock-event reasons sampled during a region.
 
+    NVML (read-only queries) from a thread every 10 ms, so that even a short
+    timed region has samples; nvidia-smi at 200 ms when NVML cannot be
+    loaded.  The device is found by its PCI bus id, so the sample is of the
+    GPU the process runs on whatever CUDA_VISIBLE_DEVICES says."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, interval_s: float = 0.01):
         self.idx = device_index
+        self.interval = interval_s
+        self.samples = []
+        self.thread = None
         self.proc = None
-        # the raw samples go to GITM_CLOCKS_DIR when set (kept), else to a
-        # temporary directory
-        keep = os.environ.get("GITM_CLOCKS_DIR")
-        d = keep or tempfile.mkdtemp(prefix="gitm_clocks_")
-        self.tmp = None if keep else d
-        self.path = os.path.join(d, f"clocks_rank{device_index}.csv")
+        self.nvml = None
+        self.handle = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self.nvml = pynvml
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.idx)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.idx)
 
     def start(self):
+        import threading
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.handle = self._nvml_handle()
+            self.smax = float(self.nvml.nvmlDeviceGetMaxClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+        except Exception:
+            self.handle = None
+        if self.handle is not None:
+            self.stop_flag = threading.Event()
+
+            def loop():
+                n = self.nvml
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append((float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)),
+                                             int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)),
+                                             n.nvmlDeviceGetPowerUsage(self.handle) / 1e3))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(self.interval)
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
+        try:
+            self.tmp = tempfile.mkdtemp(prefix="gitm_clocks_")
+            self.path = os.path.join(self.tmp, "clocks.csv")
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader",
@@ -119,15 +166,23 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
-        try:
-            return self._read()
-        finally:
-            if self.tmp:
-                shutil.rmtree(self.tmp, ignore_errors=True)
-
-    def _read(self) -> dict:
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            sm = [a for a, _, _ in self.samples]
+            reasons = sorted({name for _, r, _ in self.samples for name, bit in self.REASONS if r & bit})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(sm),
+                    "power_w_max": max((p for _, _, p in self.samples), default=None),
+                    "source": f"NVML every {1e3 * self.interval:g} ms"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
+        try:
+            return self._read_smi()
+        finally:
+            shutil.rmtree(self.tmp, ignore_errors=True)
+
+    def _read_smi(self) -> dict:
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -150,7 +205,7 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi every 200 ms"}
 
 
 # ---------------------------------------------------------------- helpers
@@ -203,26 +258,57 @@ def measure_fp64_peak(torch, device) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_baseline(m, seconds: float, threads: int | None = None, solver: str = "rusanov") -> dict:
+def workload_name(deg: float, n_cols: int, n_alts: int, solver: str) -> str:
+    """config.workload, the same string in both arms."""
+    return f"globe {deg:g} deg, {n_cols} columns x {n_alts} alts, {SOLVER_NAMES[solver]}, dt 2 s"
+
+
+def cpu_oracle_rates(m, seconds_per_call: float, n_calls: int, n_warm: int, solver: str = "rusanov",
+                     threads: int | None = None):
     """The oracle (CPU restatement of the reference) on the host cores on a
-    bounded sample: the first S columns of the globe, one step each call."""
+    bounded sample of the workload: the first S columns, one RK4 step per
+    call, S sized so that a call takes about seconds_per_call.  Every call
+    advances a fresh copy made (and first touched) outside the timed region;
+    n_warm untimed calls come first.  Returns the rates of the timed calls
+    and a description of the sample.  The same procedure serves the
+    cpu_baseline of our arm and the reference arm."""
     from gitm_b200.parallel import shard_member
     from oracle import oracle
 
+    try:
+        import torch
+        torch.set_num_threads(1)  # torch's own CPU pool stays idle beside the oracle's threads
+    except Exception:
+        pass
     threads = threads or os.cpu_count() or 1
     p = solver_params(solver)
     probe = shard_member(m, 0, max(1, m.n_cols // (64 * threads)))
+    work = probe.copy()
     t0 = time.perf_counter()
-    oracle.advance(probe.copy(), p, DT, 1, nthreads=threads)
+    oracle.advance(work, p, DT, 1, nthreads=threads)
     rate = probe.n_cols / max(time.perf_counter() - t0, 1e-6)
-    n = int(min(m.n_cols, max(threads, rate * seconds)))
-    sample = shard_member(m, 0, max(1, m.n_cols // n)) if n < m.n_cols else m.copy()
-    t0 = time.perf_counter()
-    oracle.advance(sample, p, DT, 1, nthreads=threads)
-    el = time.perf_counter() - t0
-    return {"value": sample.n_cols / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample.n_cols} of {m.n_cols} columns x 1 step (nAlts {m.n_alts}), "
-                      f"C++ oracle -O3, {threads} threads, {el:.1f} s"}
+    n = int(min(m.n_cols, max(threads, rate * seconds_per_call)))
+    sample = shard_member(m, 0, max(1, m.n_cols // n)) if n < m.n_cols else m
+    rates, els = [], []
+    for i in range(n_warm + n_calls):
+        work = sample.copy()
+        t0 = time.perf_counter()
+        oracle.advance(work, p, DT, 1, nthreads=threads)
+        el = time.perf_counter() - t0
+        if i >= n_warm:
+            rates.append(sample.n_cols / el)
+            els.append(el)
+    desc = (f"{sample.n_cols} of {m.n_cols} columns x 1 step (nAlts {m.n_alts}), C++ oracle -O3, "
+            f"{threads} threads, median of {n_calls} calls of {statistics.median(els):.2f} s after "
+            f"{n_warm} untimed")
+    return rates, desc, threads
+
+
+def cpu_baseline(m, seconds: float, solver: str = "rusanov") -> dict:
+    """cpu_baseline of our arm: the oracle on the host cores, one untimed
+    call and five timed ones of about seconds / 5 each, the median."""
+    rates, desc, threads = cpu_oracle_rates(m, max(seconds / 5.0, 0.5), 5, 1, solver)
+    return {"value": statistics.median(rates), "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -233,22 +319,15 @@ def run_reference(args):
     from gitm_b200 import synthetic
 
     m = synthetic.globe_member(args.deg, args.deg, n_alts=args.n_alts, seed=0)
-    vals = []
-    per_step = args.cpu_seconds / max(1, args.steps + args.warmup)
-    per_step = max(per_step, 1.0)
-    cb = None
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(m, min(per_step, 10.0), solver=args.solver)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals) if vals else cb["value"]
-    cb["value"] = v
+    per_call = min(max(args.cpu_seconds / max(1, args.steps + args.warmup), 0.5), 2.0)
+    rates, desc, threads = cpu_oracle_rates(m, per_call, max(args.steps, 1), args.warmup, args.solver)
+    v = statistics.median(rates)
+    cb = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * m.n_cols / v,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded)",
-           "config": {"workload": f"globe {args.deg} deg, {m.n_cols} columns x {args.n_alts} alts, "
-                                  f"{SOLVER_NAMES[args.solver]}, dt 2 s",
+           "config": {"workload": workload_name(args.deg, m.n_cols, args.n_alts, args.solver),
                       "parallelism": "host threads"},
            "cpu_baseline": cb,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -256,6 +335,71 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- our arm
+STATE_NAMES = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel")
+
+
+class GraphSteps:
+    """Graph-captured steps of a plan: a graph of `chunk` steps (and one of
+    the remainder, so that exactly `steps` steps are timed), replayed with the
+    member's input state restored between replays outside the timed region
+    (a vertical-only column has no damping and its waves grow without the
+    rest of GITM, so long runs time the same physical regime)."""
+
+    def __init__(self, torch, plan, members, dev, steps: int, chunk: int = CHUNK):
+        self.torch, self.plan, self.dev = torch, plan, dev
+        self.snap = [{k: d.tensors[k].clone() for k in STATE_NAMES} for d in members]
+        self.members = members
+        self.chunk = min(steps, chunk)
+        self.n_full, rem = divmod(steps, self.chunk)
+        self.cap = torch.cuda.Stream(dev)
+        self.cap.wait_stream(torch.cuda.current_stream(dev))
+        self.graphs = [(self._capture(self.chunk), self.chunk)] * self.n_full
+        if rem:
+            self.graphs.append((self._capture(rem), rem))
+        torch.cuda.synchronize()
+
+    def _capture(self, n):
+        g = self.torch.cuda.CUDAGraph()
+        with self.torch.cuda.stream(self.cap):
+            with self.torch.cuda.graph(g, stream=self.cap):
+                self.plan.advance(DT, n, stream=self.cap)
+        return g
+
+    def restore(self):
+        for d, sn in zip(self.members, self.snap):
+            for k in STATE_NAMES:
+                d.tensors[k].copy_(sn[k])
+
+    def launches(self) -> int:
+        return sum(self.plan.launch_count(n) for _, n in self.graphs)
+
+    def run(self, graphs=None):
+        """Device seconds of the replays (CUDA events on the capture stream)."""
+        torch = self.torch
+        el = 0.0
+        for g, _ in (graphs or self.graphs):
+            self.restore()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(self.cap):
+                e0.record(self.cap)
+                g.replay()
+                e1.record(self.cap)
+            e1.synchronize()
+            el += e0.elapsed_time(e1) / 1e3
+        return el
+
+    def sustained(self, seconds: float, clocks):
+        """Replays of the chunk graph for at least `seconds` of device time:
+        (steps, device seconds, clock record)."""
+        clocks.start()
+        el, steps = 0.0, 0
+        while el < seconds:
+            el += self.run(self.graphs[:1])
+            steps += self.graphs[0][1]
+        return steps, el, clocks.stop()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -267,7 +411,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    from gitm_b200 import abi, synthetic
+    from gitm_b200 import synthetic
     from gitm_b200 import vertical as V
 
     m = synthetic.globe_member(args.deg, args.deg, n_alts=args.n_alts, seed=rank)
@@ -276,7 +420,6 @@ def run_ours(args):
     ctx = V.VerticalContext(p, device=local)
     dm = V.device_member(m, device=dev)
     plan = V.Plan(ctx, [dm])
-    stream = torch.cuda.current_stream(dev)
 
     # -- plain per-step drop-in (default launch shape, one synchronous call per step)
     plain = None
@@ -304,52 +447,22 @@ def run_ours(args):
     elif not args.no_autotune:
         plan.autotune(DT, min(args.steps, 8))
     cfg = plan.config
-    # snapshot of the input state: every CHUNK steps the state is restored
-    # outside the timed region, so long runs time the same physical regime
-    # (a vertical-only column has no damping and its waves grow without the
-    # rest of GITM)
-    names = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel")
-    snap = {k: dm.tensors[k].clone() for k in names}
-
-    def restore():
-        for k in names:
-            dm.tensors[k].copy_(snap[k])
-
-    plan.advance(DT, max(args.warmup, 1), stream=stream)
+    gs = GraphSteps(torch, plan, [dm], dev, args.steps)
+    for _ in range(max(args.warmup, 1)):  # W untimed warm-up replays of the timed graphs
+        gs.run(gs.graphs[:1])
     torch.cuda.synchronize()
     plan.check()
-    restore()
-    chunk = min(args.steps, CHUNK)
-    graph = torch.cuda.CUDAGraph()
-    cap = torch.cuda.Stream(dev)
-    cap.wait_stream(stream)
-    with torch.cuda.stream(cap):
-        with torch.cuda.graph(graph, stream=cap):
-            plan.advance(DT, chunk, stream=cap)
-    torch.cuda.synchronize()
-    n_rep = -(-args.steps // chunk)
-    launches = plan.launch_count(chunk) * n_rep
+    launches = gs.launches()
 
     clocks = ClockSampler(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    el = 0.0
-    for _ in range(n_rep):
-        restore()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(cap):
-            e0.record(cap)
-            graph.replay()
-            e1.record(cap)
-        e1.synchronize()
-        el += e0.elapsed_time(e1) / 1e3
+    el = gs.run()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    steps_done = n_rep * chunk
+    steps_done = sum(n for _, n in gs.graphs)
     if world > 1:
         t = torch.tensor([el], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -359,42 +472,22 @@ def run_ours(args):
     total_cs = n_cols * steps_done * world
     value = total_cs / el
 
+    # -- the same replays for at least args.sustained seconds (clocks sampled)
+    sus = None
+    if args.sustained > 0:
+        s_steps, s_el, s_clk = gs.sustained(args.sustained, ClockSampler(local))
+        sus = {"value": n_cols * s_steps / s_el, "unit": UNIT, "steps": s_steps, "device_seconds": s_el,
+               "clocks": s_clk, "how": "the timed graph replayed for >= %g s of device time" % args.sustained}
+        st2, nb2 = plan.status(clear=True)
+        st, nbad = st | st2, max(nbad, nb2)
+    gs.restore()
+    del gs
+
     # -- end to end through the host-pointer C ABI (pinned host buffers)
-    e2e = None
+    e2e = e2e_opt = None
     if args.e2e_steps > 0:
-        # the arrays advance_vertical reads and writes (advance_vertical.f90:
-        # 80-217); Gamma, MeanMajorMass, TempUnit and cMax are the device's
-        # own producers here (compute_coefficients = 1), not copied
-        pinned = m.copy()
-        pinned.gamma = pinned.mean_major_mass = pinned.temp_unit = pinned.cmax = None
-        bufs = {}
-        for name, arr in pinned.arrays():
-            t = torch.from_numpy(arr).pin_memory()
-            bufs[name] = t
-            setattr(pinned, name, t.numpy())
-        h2d = sum(getattr(pinned, k).nbytes for k in ("ndensity_s", "idensity_s", "rho", "temperature",
-                                                        "velocity", "vert_vel", "ivel_up", "eddy",
-                                                        "cos_lat", "sza", "mlat"))
-        d2h = sum(getattr(pinned, k).nbytes for k in ("ndensity_s", "idensity_s", "rho", "temperature",
-                                                        "velocity", "vert_vel", "log_ns", "ndensity"))
-        V.advance_vertical_all_host(ctx, [pinned], DT, 1)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            V.advance_vertical_all_host(ctx, [pinned], DT, 1)
-        torch.cuda.synchronize()
-        ee = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([ee], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ee = float(t.item())
-        e2e = {"value": n_cols * args.e2e_steps * world / ee, "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "how": "gitm_vert_advance_native_host per step: the pinned host arrays advance_vertical "
-                      "reads copied in, stepped, the arrays it writes copied out (16 chunks, copies in / "
-                      "steps / copies out on three streams); wall clock"}
+        e2e = e2e_leg(torch, V, ctx, m, args.e2e_steps, world, dev, optional_outputs=False)
+        e2e_opt = e2e_leg(torch, V, ctx, m, args.e2e_steps, world, dev, optional_outputs=True)
 
     if rank == 0:
         flops_cs = opcount(args.n_alts, args.solver)
@@ -414,7 +507,8 @@ def run_ours(args):
                 "frac": achieved / fp64_peak,
                 "traffic": None if traffic is None else traffic * cs_launch,
                 "kernel": "vert_step_kernel",
-                "peak_source": "FP64 DGEMM (cuBLAS via torch.matmul 8192^3) measured in this run",
+                "peak_source": "FP64 DGEMM (cuBLAS via torch.matmul 8192^3) measured in this run "
+                               "(MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_column_step": flops_cs,
                 "flop_convention": "add/mul/div/sqrt = 1, exp/log/pow = 20 (oracle count, dead code excluded)"}
         hbm = None
@@ -427,34 +521,140 @@ def run_ours(args):
                "steps": steps_done, "warmup": args.warmup,
                "ms_per_step": 1e3 * el / steps_done, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-               "config": {"workload": f"globe {args.deg} deg, {n_cols} columns x {args.n_alts} alts "
-                                      f"per GPU, {SOLVER_NAMES[args.solver]}, dt 2 s",
+               "config": {"workload": workload_name(args.deg, n_cols, args.n_alts, args.solver),
                           "columns_per_gpu": n_cols, "n_alts": args.n_alts,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                           "l2": "state larger than L2 (no flush needed)",
                           "launch": {"threads": cfg.threads, "cols_per_cta": cfg.cols_per_cta,
                                      "steps_per_launch": cfg.steps_per_launch,
                                      "ctas_per_sm": cfg.ctas_per_sm, "graph": True,
-                                     "graph_steps": chunk, "state_restored_every": chunk}},
+                                     "graph_steps": min(args.steps, CHUNK),
+                                     "state_restored_every": min(args.steps, CHUNK)}},
                "clocks": clk, "gpu_launches": launches, "status": {"or": st, "bad_columns": nbad},
                "roofline": roof, "roofline_hbm": hbm, "cpu_baseline": cb, "e2e": e2e,
-               "plain": plain}
-        print(json.dumps(out))
+               "e2e_with_optional_outputs": e2e_opt, "plain": plain, "sustained": sus}
     plan.close()
+    del dm
+    torch.cuda.empty_cache()
+    if rank == 0:
+        if world == 1 and not args.no_extras:
+            out["extras"] = run_extras(args, m)
+        print(json.dumps(out))
     ctx.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
 
 
+def e2e_leg(torch, V, ctx, m, n_steps: int, world: int, dev, optional_outputs: bool) -> dict:
+    """The same metric end to end through the host-pointer C ABI
+    (gitm_vert_advance_native_host) with pinned host arrays: every step copies
+    in the arrays advance_vertical reads, steps and copies out the state it
+    writes (and LogNS / NDensity with optional_outputs); wall clock."""
+    import torch.distributed as dist
+    pinned = m.copy()
+    # Gamma, MeanMajorMass, TempUnit and cMax are the device's own producers
+    # here (compute_coefficients = 1), not copied
+    pinned.gamma = pinned.mean_major_mass = pinned.temp_unit = pinned.cmax = None
+    if not optional_outputs:
+        pinned.log_ns = pinned.ndensity = None
+    for name, arr in list(pinned.arrays()):
+        t = torch.from_numpy(arr).pin_memory()
+        setattr(pinned, name, t.numpy())
+    ins = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel", "ivel_up", "eddy",
+           "cos_lat", "sza", "mlat")
+    outs = STATE_NAMES + (("log_ns", "ndensity") if optional_outputs else ())
+    h2d = sum(getattr(pinned, k).nbytes for k in ins)
+    d2h = sum(getattr(pinned, k).nbytes for k in outs)
+    V.advance_vertical_all_host(ctx, [pinned], DT, 1)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_steps):
+        V.advance_vertical_all_host(ctx, [pinned], DT, 1)
+    torch.cuda.synchronize()
+    ee = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([ee], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ee = float(t.item())
+    return {"value": m.n_cols * n_steps * world / ee, "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "how": "gitm_vert_advance_native_host per step: the pinned host arrays advance_vertical "
+                   "reads copied in, stepped, the state it writes copied out"
+                   + (" with the optional LogNS and NDensity outputs" if optional_outputs else "")
+                   + " (16 chunks, copies in / steps / copies out on three streams); wall clock"}
+
+
+def ausm_report(args, m) -> dict:
+    """The same globe and metric with the AUSM solver (UseAUSMSolver = T):
+    autotuned launch shape, exactly args.steps graph-captured steps."""
+    import torch
+
+    from gitm_b200 import vertical as V
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctx = V.VerticalContext(solver_params("ausm"), device=dev.index)
+    dm = V.device_member(m, device=dev)
+    plan = V.Plan(ctx, [dm])
+    plan.autotune(DT, min(args.steps, 8))
+    cfg = plan.config
+    gs = GraphSteps(torch, plan, [dm], dev, args.steps)
+    gs.run(gs.graphs[:1])
+    plan.check()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    el = gs.run()
+    clk = clocks.stop()
+    steps = sum(n for _, n in gs.graphs)
+    launches = gs.launches()
+    st, nbad = plan.status(clear=True)
+    plan.close()
+    ctx.close()
+    flops = opcount(args.n_alts, "ausm")
+    value = m.n_cols * steps / el
+    return {"metric": "column-steps/s, AUSM solver", "value": value, "unit": UNIT, "steps": steps,
+            "ms_per_step": 1e3 * el / steps,
+            "config": {"workload": workload_name(args.deg, m.n_cols, args.n_alts, "ausm"),
+                       "launch": {"threads": cfg.threads, "steps_per_launch": cfg.steps_per_launch,
+                                  "ctas_per_sm": cfg.ctas_per_sm, "graph": True}},
+            "roofline": {"bound": "fp64", "achieved": flops * value / 1e12, "unit": "TFLOP/s",
+                         "flops_per_column_step": flops,
+                         "how": "frac against the FP64 DGEMM peak of the main line"},
+            "clocks": clk, "gpu_launches": launches, "status": {"or": st, "bad_columns": nbad}}
+
+
+def run_extras(args, m) -> dict:
+    """The rest of the reference's headline metric, measured in the default
+    run: the AUSM solver on the same globe, the adjoint rollout (adjoint /
+    forward cost, peak memory) and the uneven ensemble against the per-member
+    plain loop.  Each is bounded to well under a minute of work."""
+    out = {}
+    for name, fn in (("ausm", lambda: ausm_report(args, m)),
+                     ("adjoint", lambda: run_adjoint(args, fd_directions=args.extra_fd)),
+                     ("ensemble", lambda: run_ensemble(args))):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as exc:  # an extra that fails is reported, not fatal to the line
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        if isinstance(out[name], dict):
+            out[name]["wall_seconds"] = time.perf_counter() - t0
+        __import__("torch").cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- adjoint
-def run_adjoint(args):
+def run_adjoint(args, fd_directions: int | None = None):
     """Adjoint rollout: J = sum_c w_c log(n_O / n_N2) at 400 km after
     adj_steps steps of the adj_deg globe, w_c ~ U[0, 1]; gradients with
     respect to the initial state, the eddy coefficient and the per-column
     heating factor through gitm_b200.adjoint.rollout (checkpoints every
     adj_every steps).  Reports forward and backward device time, their ratio
-    per step, the peak device memory and a finite-difference check."""
+    per step, the peak device memory and a finite-difference check.  Returns
+    the report (rank 0) or None."""
+    if fd_directions is None:
+        fd_directions = args.fd_directions
     import torch
 
     from gitm_b200 import abi, synthetic
@@ -580,7 +780,7 @@ def run_adjoint(args):
 
     def _fd_errors(per_column_J, grads):
         errs = []
-        for trial in range(args.fd_directions):
+        for trial in range(fd_directions):
             col = int(torch.randint(0, n_cols, (1,), generator=gen, device=dev))
             d = {}
             for k in names:
@@ -606,7 +806,7 @@ def run_adjoint(args):
         return np.array(errs)
 
     eps = 1e-7
-    if args.fd_directions > 0:
+    if fd_directions > 0:
         grads1 = grads_once(1)[0]
         errs1 = fd_errors(1, grads1)
         errs = fd_errors(args.adj_steps, grads)
@@ -650,7 +850,8 @@ def run_adjoint(args):
                           "subtracted; the limiter's kinks are dense (a 1e-7 perturbation of one "
                           "column flips branches within a few steps), so rollout differences mix "
                           "branches; the branch-exact check is tests/test_gpu_adjoint.py"}}
-        print(json.dumps(out))
+        return out
+    return None
 
 
 # ---------------------------------------------------------------- ensemble
@@ -720,7 +921,7 @@ def run_ensemble(args):
     t_plain = (time.perf_counter() - t0) / args.ens_plain_steps
     restore()
     plan = V.Plan(ctx, dms)
-    cfg = plan.autotune(DT, 4)
+    cfg = plan.autotune(DT, 2)
     restore()
     chunk = min(args.ens_steps, CHUNK)
     graph = torch.cuda.CUDAGraph()
@@ -769,7 +970,9 @@ def run_ensemble(args):
                               "ms_per_step": 1e3 * t_plain,
                               "how": "gitm_vert_advance_native per member per step (plan built each call), "
                                      "wall clock"}}
-        print(json.dumps(out))
+        out["batched_over_plain"] = out["value"] / out["plain_loop"]["value"]
+        return out
+    return None
 
 
 def measured_hbm_peak() -> float:
@@ -915,10 +1118,14 @@ def main():
         run_horizontal(args)
         return
     if args.ensemble:
-        run_ensemble(args)
+        out = run_ensemble(args)
+        if out:
+            print(json.dumps(out))
         return
     if args.adjoint:
-        run_adjoint(args)
+        out = run_adjoint(args)
+        if out:
+            print(json.dumps(out))
     elif args.impl == "reference":
         run_reference(args)
     else:
