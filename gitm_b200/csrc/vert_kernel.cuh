@@ -152,9 +152,11 @@ __device__ __forceinline__ double lane_seq_sum(double v, int n) {
 
 // ------------------------------------------------------------ boundaries
 // set_vertical_bcs (Earth), set_vertical_bcs.Earth.f90:8-652, for one column.
-// part 1 = lower boundary (cells -1, 0), part 2 = upper boundary (nAlts+1,
-// nAlts+2), part 3 = both; the two halves touch disjoint cells and can run on
-// different warps.  Executed by a full warp, lanes over species / ions.
+// part 1 = the lower boundary (cells -1, 0) with the neutral densities and
+// LogRho of the upper ghost cells, part 2 = the rest of the upper boundary
+// (nAlts+1, nAlts+2: winds, temperature, ions), part 3 = both; the two parts
+// touch disjoint cells and fields and can run on different warps.  Executed
+// by a full warp, lanes over species / ions.
 //
 // Where the reference goes through exp and back through log with a factor
 // that is exactly 1 (Temp(-1) = Temp(0) and Temp(nAlts+1:nAlts+2) =
@@ -255,22 +257,39 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
       c.ion(s, -1) = v;
     }
     __syncwarp();
-    // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1
+    // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1; with
+    // them the upper boundary's hydrostatic neutrals (lines 471-486,
+    // Temp(nA+1:nA+2) = Temp(nA)) and its LogRho (lines 598-604), which read
+    // only interior cells and these ghosts: the warp of the upper half keeps
+    // the ion chain alone, and the four LogRho ghosts share one log
     {
-      double m0 = 0.0, m1 = 0.0, t0 = 0.0, t1 = 0.0;
+      double m0 = 0.0, m1 = 0.0, t0 = 0.0, t1 = 0.0, mu1 = 0.0, mu2 = 0.0;
       if (s < NS) {
+        const double T = x(F_T, nA);
+        const double den = 0.5 * (T + T) * KB;
+        const double ish1 = (-0.5 * (sc[SC_EG + 3] + sc[SC_EG + 2])) * c_k.mass[s] / den;
+        const double ish2 = (-0.5 * (sc[SC_EG + 4] + sc[SC_EG + 3])) * c_k.mass[s] / den;
+        const double l1 = x(F_LNS + s, nA) - ish1 * sc[SC_DAF + 4];
+        const double l2 = l1 - ish2 * sc[SC_DAF + 5];
+        x(F_LNS + s, nA + 1) = l1;
+        x(F_LNS + s, nA + 2) = l2;
         m0 = c_k.mass[s] * exp(x(F_LNS + s, 0));
         m1 = c_k.mass[s] * exp(x(F_LNS + s, -1));
+        mu1 = c_k.mass[s] * exp(l1);
+        mu2 = c_k.mass[s] * exp(l2);
         t0 = m0 * x(F_W + s, 0);
         t1 = m1 * x(F_W + s, -1);
       }
       const double r0 = lane_seq_sum(m0, NS), r1 = lane_seq_sum(m1, NS);
       const double v0 = lane_seq_sum(t0, NS), v1 = lane_seq_sum(t1, NS);
-      // lane 0 takes cell 0, lane 1 cell -1: one log and one division for both
-      if (s < 2) {
-        const double r = s ? r1 : r0;
-        x(F_LRHO, -s) = log(r);
-        x(F_VU, -s) = (s ? v1 : v0) / r;
+      const double ru1 = lane_seq_sum(mu1, NS), ru2 = lane_seq_sum(mu2, NS);
+      // lanes 0..3 take cells 0, -1, nAlts+1, nAlts+2: one log for the four
+      // and one division for the two lower ones
+      if (s < 4) {
+        const double r = (s == 0) ? r0 : (s == 1) ? r1 : (s == 2) ? ru1 : ru2;
+        const int cell = (s < 2) ? -s : nA + s - 1;
+        x(F_LRHO, cell) = log(r);
+        if (s < 2) x(F_VU, -s) = (s ? v1 : v0) / r;
       }
     }
     // lines 364-376
@@ -301,13 +320,8 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
       }
       x(F_W + s, nA + 1) = w1;
       x(F_W + s, nA + 2) = w2;
-      // lines 471-486: hydrostatic neutrals, Temp(nA+1:nA+2) = Temp(nA)
-      const double T = x(F_T, nA);
-      const double ish1 = (-0.5 * (sc[SC_EG + 3] + sc[SC_EG + 2])) * c_k.mass[s] / (0.5 * (T + T) * KB);
-      const double ish2 = (-0.5 * (sc[SC_EG + 4] + sc[SC_EG + 3])) * c_k.mass[s] / (0.5 * (T + T) * KB);
-      const double l1 = x(F_LNS + s, nA) - ish1 * sc[SC_DAF + 4];
-      x(F_LNS + s, nA + 1) = l1;
-      x(F_LNS + s, nA + 2) = l1 - ish2 * sc[SC_DAF + 5];
+      // the hydrostatic neutrals (lines 471-486) are formed with the lower
+      // boundary (part 1)
     }
     if (s == 10) {
       const double v = x(F_VU, nA);
@@ -319,22 +333,33 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
       x(F_T, nA + 1) = x(F_T, nA);
       x(F_T, nA + 2) = x(F_T, nA);
     }
-    // lines 497-501: TEC of the first ion
+    // lines 497-501: TEC of the first ion; with UseImprovedIonAdvection,
+    // the scan for negative values of check_for_negative_densities (lines
+    // 608-649, which acts only when a value in nAlts-5 .. nAlts+2 is
+    // negative) and, in the same block so that their latencies overlap, the
+    // logs the extrapolation of lines 503-596 takes when no value is
+    // negative: lg[7 s + j] = log(ion s at nAlts+2-j), j = 0..6 (the ghost
+    // nAlts+2 and the cells nAlts+1 .. nAlts-4), 63 logs, two per lane
     double tp = 0.0;
-    for (int i = 1 + lane; i <= nA; i += 32) {
-      const double v = c.ion(0, i);
-      tp += c.dAF(i) * (improved ? v : exp(v));
+    bool neg = false;
+    double* lg = c.col + c.L.DL;  // scratch: the slopes are dead during the BCs
+    if (improved) {
+      for (int i = 1 + lane; i <= nA; i += 32) tp += c.dAF(i) * c.ion(0, i);
+      if (s < NI)
+        for (int q = nA - 5; q <= nA + 2; ++q) neg = neg || (c.ion(s, q) < 0.0);
+      for (int q = lane; q < NI * 7; q += 32) {
+        const int si = q / 7, j = q - si * 7;
+        lg[q] = log(c.ion(si, nA + 2 - j));
+      }
+    } else {
+      for (int i = 1 + lane; i <= nA; i += 32) tp += c.dAF(i) * exp(c.ion(0, i));
     }
     for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
     // TEC / 1e16 < MinTEC (1e16 is exact in binary64)
     const bool hold = (tp < prm.min_tec * 1e16) && (sc[SC_PLASMA] != 0.0);
     const double* bu = sc + SC_BCC + 10;  // upper mesh coefficients, nA+1 then nA+2
-    // check_for_negative_densities (lines 608-649) can only act when a value
-    // in nAlts-5 .. nAlts+2 is negative
-    bool neg = false;
-    if (improved && s < NI)
-      for (int q = nA - 5; q <= nA + 2; ++q) neg = neg || (c.ion(s, q) < 0.0);
     const bool anyneg = __any_sync(0xffffffffu, neg);
+    __syncwarp();
     if (!improved) {
       if (s < NI && !hold) {
         #pragma unroll
@@ -381,17 +406,11 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
         }
       }
     } else if (!hold) {
-      // no negative value: the logs of the 9 ions x 6 cells are independent,
-      // so the warp takes them two per lane; the second cell reuses four.
-      double* lg = c.col + c.L.DL;  // scratch: the slopes are dead during the BCs
-      for (int q = lane; q < NI * 6; q += 32) {
-        const int si = q / 6, j = q - si * 6;
-        lg[q] = log(c.ion(si, nA + 1 - j));
-      }
-      __syncwarp();
+      // no negative value: the logs taken above (the second cell reuses
+      // four of the first's)
       double n1 = 0.0;
       if (s < NI) {
-        const double* n = lg + s * 6;
+        const double* n = lg + s * 7 + 1;  // n[k] = log(ion at nAlts+1-k)
         const double* C = bu;
         double dn = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
         const double lim = -(0.001 * n[0] / sc[SC_DAF + 3]);
@@ -400,7 +419,7 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
         c.ion(s, nA + 1) = exp(y);
         // cell nAlts+2: the log of its own ghost, and y for the log of the
         // value just set (log(exp(y)) in the reference, y to rounding)
-        const double g0 = log(c.ion(s, nA + 2));
+        const double g0 = lg[s * 7];
         n1 = y;
         const double* D = bu + 5;
         double dn2 = D[0] * n1 + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
@@ -409,17 +428,8 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
         c.ion(s, nA + 2) = exp(n1 + dn2 * sc[SC_DAF + 5]);
       }
     }
-    __syncwarp();
-    // lines 598-604
-    {
-      double m1 = 0.0, m2 = 0.0;
-      if (s < NS) {
-        m1 = c_k.mass[s] * exp(x(F_LNS + s, nA + 1));
-        m2 = c_k.mass[s] * exp(x(F_LNS + s, nA + 2));
-      }
-      const double r1 = lane_seq_sum(m1, NS), r2 = lane_seq_sum(m2, NS);
-      if (s < 2) x(F_LRHO, nA + 1 + s) = log(s ? r2 : r1);
-    }
+    // LogRho of nAlts+1, nAlts+2 (lines 598-604) is formed with the lower
+    // boundary (part 1)
   }
   __syncwarp();
 }
