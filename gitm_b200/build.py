@@ -44,11 +44,12 @@ def instances() -> list[tuple[str, list[str]]]:
     text = open(os.path.join(CSRC, "vert_instances.h")).read()
     body = text[text.index("#define GV_STEP_INSTANCES(X)"):].split("\n\n", 1)[0]
     out = []
-    for m in re.finditer(r"X\((\w+),\s*(\d+),\s*(\d+),\s*(\d+),\s*(true|false),\s*(\d+),\s*(true|false),\s*(\d+)\)",
-                         body):
-        gid, io, nt, minb, acc, solver, save, na = m.groups()
+    for m in re.finditer(r"X\((\w+),\s*(\d+),\s*(\d+),\s*(\d+),\s*(true|false),\s*(\d+),\s*(true|false),\s*(\d+),"
+                         r"\s*(true|false)\)", body):
+        gid, io, nt, minb, acc, solver, save, na, og = m.groups()
         out.append((gid, [f"-DGV_ID={gid}", f"-DGV_IO={io}", f"-DGV_NT={nt}", f"-DGV_MINB={minb}",
-                          f"-DGV_ACC={acc}", f"-DGV_SOLVER={solver}", f"-DGV_SAVE={save}", f"-DGV_NA={na}"]))
+                          f"-DGV_ACC={acc}", f"-DGV_SOLVER={solver}", f"-DGV_SAVE={save}", f"-DGV_NA={na}",
+                          f"-DGV_OG={og}"]))
     if not out:
         raise RuntimeError("no step-kernel instances found in vert_instances.h")
     return out

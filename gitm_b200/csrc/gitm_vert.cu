@@ -75,8 +75,9 @@ struct GitmVertPlan {
   Tile* d_tiles = nullptr;
   size_t smem = 0;
   int grid = 0;                 // CTAs per launch for the current cfg
-  double* d_scratch = nullptr;  // RK accumulators of persistent CTAs
+  double* d_scratch = nullptr;  // RK accumulators (and Orig) of persistent CTAs
   size_t scratch_doubles = 0;
+  int64_t scratch_per_cta = 0;  // doubles of one CTA's scratch slot
   int max_nalts = 0, min_nalts = 1 << 30;
   // adjoint launch (built on the first gitm_vert_plan_adjoint)
   bool adj_ready = false;
@@ -235,14 +236,24 @@ static void grid_coefs(int nA, const double* alt, const double* grav, const doub
 // where the RK accumulator lives.  The small CTAs keep it in a per-CTA slot
 // of global scratch (L2-resident under their persistent grid) so that two or
 // three CTAs share an SM and overlap each other's barrier phases.
-struct Shape { int threads, min_blocks; bool acc_global; };
-static const Shape kShapes[] = {{128, 3, true}, {160, 2, true}, {192, 2, true},
-                                {256, 1, false}, {320, 1, false}, {384, 1, false}};
-static const int kThreadChoices[] = {128, 160, 192, 256, 320, 384};
+// The 512-thread shape also keeps Orig in its scratch slot (orig_global):
+// 8 columns of 50 altitudes then fit the shared memory of an SM, 16 warps at
+// 128 registers.
+struct Shape { int threads, min_blocks; bool acc_global, orig_global; };
+static const Shape kShapes[] = {{128, 3, true, false}, {160, 2, true, false}, {192, 2, true, false},
+                                {256, 1, false, false}, {320, 1, false, false}, {384, 1, false, false},
+                                {512, 1, true, true}};
+static const int kThreadChoices[] = {128, 160, 192, 256, 320, 384, 512};
 
 static bool acc_global(int threads) {
   for (const Shape& s : kShapes)
     if (s.threads == threads) return s.acc_global;
+  return false;
+}
+
+static bool orig_global(int threads) {
+  for (const Shape& s : kShapes)
+    if (s.threads == threads) return s.orig_global;
   return false;
 }
 
@@ -256,7 +267,7 @@ struct StepInstance {
   cudaError_t (*consts)(const Consts&);
 };
 static const StepInstance kInstances[] = {
-#define GV_TABLE_ENTRY(id, IO, NT, MINB, ACC, SOLVER, SAVE, NA) \
+#define GV_TABLE_ENTRY(id, IO, NT, MINB, ACC, SOLVER, SAVE, NA, OG) \
   {IO, NT, SOLVER, SAVE, NA, step_kernel_##id, step_consts_##id},
     GV_STEP_INSTANCES(GV_TABLE_ENTRY)
 #undef GV_TABLE_ENTRY
@@ -396,7 +407,7 @@ static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int
   int nc = cfg.cols_per_cta > 0 ? cfg.cols_per_cta : cfg.threads / nA;
   nc = std::min(nc, cfg.threads / 32);  // one BC warp per column
   nc = std::min(nc, cfg.threads / nA);  // every interior cell has a thread
-  while (nc > 1 && smem_bytes(nA, nc, solver) > ctx->max_smem) --nc;
+  while (nc > 1 && smem_bytes(nA, nc, solver, orig_global(cfg.threads)) > ctx->max_smem) --nc;
   return std::max(nc, 1);
 }
 
@@ -406,13 +417,16 @@ static int build_tiles(GitmVertPlan* P) {
     return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built for solver %d", P->cfg.threads, P->solver);
   P->tiles.clear();
   P->smem = 0;
+  const bool og = orig_global(P->cfg.threads);
+  size_t orig_per_cta = 0;  // doubles of Orig a CTA's scratch slot holds (orig_global shapes)
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnBatch& b = P->host_members[m];
     const int nc = cols_per_cta(ctx, P->cfg, b.n_alts, P->solver);
-    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc, P->solver) > ctx->max_smem)
+    if (nc * b.n_alts > P->cfg.threads || smem_bytes(b.n_alts, nc, P->solver, og) > ctx->max_smem)
       return set_err(ctx, GITM_ERR_ARG, "nAlts %d does not fit a CTA of %d threads", b.n_alts,
                      P->cfg.threads);
-    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc, P->solver));
+    P->smem = std::max(P->smem, smem_bytes(b.n_alts, nc, P->solver, og));
+    if (og) orig_per_cta = std::max(orig_per_cta, size_t(nc) * orig_doubles(b.n_alts));
     for (int64_t c0 = 0; c0 < b.n_cols; c0 += nc) {
       Tile t;
       t.member = m;
@@ -440,9 +454,10 @@ static int build_tiles(GitmVertPlan* P) {
   }
   if (per_sm > 0) grid = std::min(grid, per_sm * ctx->num_sms);
   P->grid = std::max(grid, 1);
+  P->scratch_per_cta = int64_t(NF) * T + int64_t(orig_per_cta);
   if (acc_global(T)) {
     // at least three slots: the host-pointer path splits them over 3 streams
-    const size_t need = size_t(std::max(P->grid, 3)) * NF * T;
+    const size_t need = size_t(std::max(P->grid, 3)) * size_t(P->scratch_per_cta);
     if (need > P->scratch_doubles) {
       cudaFree(P->d_scratch);
       P->d_scratch = nullptr;
@@ -646,6 +661,7 @@ static int launch_steps(GitmVertPlan* P, double dt, int n_steps, cudaStream_t st
   kp.dt = dt;
   kp.status = P->d_status;
   kp.scratch = P->d_scratch;
+  kp.scratch_per_cta = P->scratch_per_cta;
   kp.prm = ctx->params;
   for (int done = 0; done < n_steps; done += spl) {
     kp.n_steps = std::min(spl, n_steps - done);
@@ -1241,6 +1257,7 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
     kp.dt = dt;
     kp.status = P->d_status;
     kp.scratch = P->d_scratch;
+    kp.scratch_per_cta = P->scratch_per_cta;
     kp.prm = prm;
     const int cgrid = P->d_scratch ? std::min(kp.n_tiles, P->grid) : kp.n_tiles;
     for (int done = 0; done < n_steps && kp.n_tiles > 0; done += spl) {

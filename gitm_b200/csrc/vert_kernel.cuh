@@ -55,8 +55,11 @@ enum Scalar : int {
 
 // Per-column shared-memory slot (doubles): the stage state twice (a stage
 // reads one buffer and writes the next), Orig, the limited slopes, the
-// per-cell coefficients and the column scalars.
-__host__ __device__ inline Layout make_layout(int nAlts, int solver = GITM_SOLVER_RUSANOV) {
+// per-cell coefficients and the column scalars.  orig_global: Orig is kept
+// in the CTA's slot of global scratch instead (it is read-only during a
+// step), which leaves room for more columns per SM.
+__host__ __device__ inline Layout make_layout(int nAlts, int solver = GITM_SOLVER_RUSANOV,
+                                              bool orig_global = false) {
   Layout L;
   L.nAlts = nAlts;
   L.G = nAlts + 4;
@@ -67,8 +70,8 @@ __host__ __device__ inline Layout make_layout(int nAlts, int solver = GITM_SOLVE
   L.XP0 = o; o += NPAS * NPC;
   L.X1 = o;  o += NF * G;
   L.XP1 = o; o += NPAS * NPC;
-  L.O = o;   o += NF * G;
-  L.OP = o;  o += NPAS * NPC;
+  L.O = o;   o += orig_global ? 0 : NF * G;
+  L.OP = o;  o += orig_global ? 0 : NPAS * NPC;
   L.DL = o;  o += L.nsl * (nAlts + 2);
   L.TU = o;  o += G;
   L.CM = o;  o += G;
@@ -82,10 +85,14 @@ __host__ __device__ inline Layout make_layout(int nAlts, int solver = GITM_SOLVE
 }
 
 // Bytes of dynamic shared memory a tile of nc columns needs.
-__host__ __device__ inline size_t smem_bytes(int nAlts, int nc, int solver = GITM_SOLVER_RUSANOV) {
-  Layout L = make_layout(nAlts, solver);
+__host__ __device__ inline size_t smem_bytes(int nAlts, int nc, int solver = GITM_SOLVER_RUSANOV,
+                                             bool orig_global = false) {
+  Layout L = make_layout(nAlts, solver, orig_global);
   return size_t(L.stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
 }
+
+// Doubles of one column's Orig (the state and its passive-ion cells).
+__host__ __device__ inline int orig_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
 
 // passive-ion cell slot: -1,0,1 -> 0..2; nAlts-5..nAlts+2 -> 3..10
 __device__ __forceinline__ int pcell(int i, int nAlts) {
@@ -664,7 +671,9 @@ struct KParams {
   int n_steps;
   double dt;
   uint32_t* status;   // one word per column (member col_offset + column)
-  double* scratch;    // RK accumulators, NF * NT doubles per CTA (ACC_GLOBAL)
+  double* scratch;    // per-CTA slots of global scratch: RK accumulators, NF * NT doubles
+                      // (ACC_GLOBAL), then with OG the Orig of the tile's columns
+  int64_t scratch_per_cta;  // doubles of one CTA's slot (OG kernels)
   GitmVertParams prm;
   // SAVE kernels (one step per launch): the gathered state and the
   // post-boundary stage states X0..X4 of every column, state s of global
@@ -682,15 +691,22 @@ struct KParams {
 // NA > 0: every member has exactly NA altitudes (the host checks), so the
 // shared-memory layout, the item mapping and the loop bounds are
 // compile-time constants; NA = 0 reads nAlts from the member.
-template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER, bool SAVE = false, int NA = 0>
+// OG (with ACC_GLOBAL): Orig lives in the CTA's slot of global scratch after
+// the accumulators (coalesced, L2-resident, read-only within a step), so a
+// column needs 8 KB less shared memory and more columns share an SM.
+template <int IO, int NT, int MINB, bool ACC_GLOBAL, int SOLVER, bool SAVE = false, int NA = 0, bool OG = false>
 __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
+  static_assert(!OG || ACC_GLOBAL, "Orig in global scratch goes with the accumulators there");
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int wid = tid >> 5;
   const GitmVertParams& prm = kp.prm;
   const double dt = kp.dt;
-  double* accg = ACC_GLOBAL ? kp.scratch + size_t(blockIdx.x) * NF * NT + tid : nullptr;
+  double* const slot = ACC_GLOBAL ? kp.scratch + size_t(blockIdx.x) * (OG ? size_t(kp.scratch_per_cta) : size_t(NF) * NT)
+                                  : nullptr;
+  double* accg = ACC_GLOBAL ? slot + tid : nullptr;
+  double* const ogb = OG ? slot + size_t(NF) * NT : nullptr;  // Orig of column cl at ogb + cl * orig_doubles
   const double inv_vert_tau = 1.0 / prm.vert_tau;  // 1 / VertTau without damping
 
   for (int tix = blockIdx.x; tix < kp.n_tiles; tix += gridDim.x) {
@@ -698,7 +714,8 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
     const DevMember& M = kp.members[tile.member];
     const int nA = (NA > 0) ? NA : M.b.n_alts;
     const int nc = tile.nc;
-    const Layout L = make_layout(nA, SOLVER);
+    const Layout L = make_layout(nA, SOLVER, OG);
+    const int operc = orig_doubles(nA);  // Orig doubles per column (OG)
     const int G = L.G;
     const int64_t ncols = M.b.n_cols;
     uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(L.stride) * nc);  // [nc] status
@@ -924,7 +941,11 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         for (int w = tid; w < nc * per; w += NT) {
           const int cl = w / per, r = w - cl * per;
           double* col = sm + size_t(L.stride) * cl;
-          col[L.O + r] = col[xo + r];
+          if constexpr (OG) {
+            ogb[size_t(cl) * operc + r] = col[xo + r];
+          } else {
+            col[L.O + r] = col[xo + r];
+          }
         }
       }
 
@@ -971,7 +992,7 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
             const int fa = ACC_GLOBAL ? 0 : f;
             // the first stage starts the accumulator: no read of the slot
             const double prev = (k == 0) ? 0.0 : ACC_GLOBAL ? accg[size_t(f) * NT] : accr[fa];
-            const double o = c.o(f, i);
+            const double o = OG ? ogb[size_t(my_cl) * operc + f * G + i + 1] : c.o(f, i);
             double a, x1;
             if constexpr (SOLVER == GITM_SOLVER_AUSM) {
               // Stage(k+2) = Stage1 + (New - state), and the final combination
@@ -1010,12 +1031,13 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           for (int w = tid; w < nc * per; w += NT) {
             const int cl = w / per, r = w - cl * per;
             double* col = sm + size_t(L.stride) * cl;
+            const double* ocol = OG ? ogb + size_t(cl) * operc : col + L.O;  // OP follows O in both
             if (r < NF * 4) {
               const int f = r >> 2, u = r & 3;
               const int g = (u < 2) ? u : nA + u;  // cells -1,0,nA+1,nA+2
-              col[nxo + f * G + g] = col[L.O + f * G + g];
+              col[nxo + f * G + g] = ocol[f * G + g];
             } else {
-              col[nxpo + r - NF * 4] = col[L.OP + r - NF * 4];
+              col[nxpo + r - NF * 4] = ocol[NF * G + r - NF * 4];
             }
           }
         }
@@ -1078,7 +1100,8 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           // started from (Orig, with this step's TempUnit): the coefficient
           // the next step reads (calc_sources.f90:26 runs after the vertical
           // advance)
-          const double pr = (c.o(F_T, i) / c.tu(i)) * exp(c.o(F_LRHO, i));
+          const double* ocol = OG ? ogb + size_t(cl) * operc : c.col + L.O;
+          const double pr = (ocol[F_T * G + i + 1] / c.tu(i)) * exp(ocol[F_LRHO * G + i + 1]);
           double kz = 0.0;
           if (pr > prm.eddy_pressure0)
             kz = prm.eddy_coef;

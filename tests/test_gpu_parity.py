@@ -138,7 +138,7 @@ def test_other_altitude_counts(torch_cuda, oracle_lib, n_alts):
     assert_state_close(out, ref, STATE)
 
 
-@pytest.mark.parametrize("threads", [256, 320, 384])
+@pytest.mark.parametrize("threads", [256, 320, 384, 512])
 def test_launch_shapes_agree(torch_cuda, oracle_lib, threads):
     p = abi.default_params()
     m = synthetic.make_member(50, 50, seed=24)
@@ -318,6 +318,6 @@ def test_autotune_leaves_state(torch_cuda):
     dm = V.device_member(m)
     plan = V.Plan(ctx, [dm])
     cfg = plan.autotune(2.0, 2)
-    assert cfg.threads in (128, 160, 192, 256, 320, 384)
+    assert cfg.threads in (128, 160, 192, 256, 320, 384, 512)
     np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
     assert plan.status() == (0, 0)
