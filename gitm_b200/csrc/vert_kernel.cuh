@@ -984,6 +984,12 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
         // result goes straight into the other buffer as Orig + c_k K_k
         // (vertical_solver_rusanov.f90:120-163,190-232,261-303,350-366)
         const int nxo = cur ? L.X0 : L.X1;
+        // the RK4 weights of this stage: accumulator a = prev + ca K (ca = 1,
+        // 2, 2, 1), next state Orig + cx K for k < 3 (cx = 1/2, 1/2, 1) and
+        // Orig + a / 6 after the last stage; a multiplication by 1 or 2 is
+        // exact, so fma(ca, K, prev) rounds like prev + ca K
+        const double ca = (k == 1 || k == 2) ? 2.0 : 1.0;
+        const double cx = (k < 2) ? 0.5 : (k == 2) ? 1.0 : 1.0 / 6.0;
         if (item) {
           ColCtx c = ctx(my_cl);
           const int i = my_i;
@@ -1006,8 +1012,8 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
                 x1 = (1.0 / 3.0) * (prev + kval);
               }
             } else {
-              a = (k == 0) ? kval : (k < 3) ? prev + 2.0 * kval : prev + kval;
-              x1 = (k < 2) ? o + 0.5 * kval : (k == 2) ? o + kval : o + (1.0 / 6.0) * a;
+              a = fma(ca, kval, prev);
+              x1 = o + cx * ((k == 3) ? a : kval);
             }
             if constexpr (ACC_GLOBAL) {
               accg[size_t(f) * NT] = a;
