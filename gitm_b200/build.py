@@ -72,6 +72,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     extra = ["-Xptxas", "-v"] if verbose else []
     jobs = [(os.path.join(CSRC, s), [], os.path.join(BUILD, s[:-3] + ".o")) for s in SOURCES]
+    # the adjoint kernel for members of 50 altitudes, in a unit of its own
+    jobs.append((os.path.join(CSRC, "vert_adjoint.cu"), ["-DGV_ADJ_NA=50"], os.path.join(BUILD, "vert_adjoint_n50.o")))
     jobs += [(os.path.join(CSRC, "vert_instance.cu"), flags, os.path.join(BUILD, f"step_{gid}.o"))
              for gid, flags in instances()]
 

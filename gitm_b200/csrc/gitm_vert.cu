@@ -361,7 +361,10 @@ int gitm_vert_create(const GitmVertParams* params, int device, GitmVertCtx** out
   Consts k;
   fill_consts(k);
   if (cudaMemcpyToSymbol(c_k, &k, sizeof k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
-  if (adjoint_set_consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
+  if (adjoint_set_consts(k) != cudaSuccess || adjoint_set_consts_n50(k) != cudaSuccess) {
+    delete ctx;
+    return GITM_ERR_CUDA;
+  }
   for (const StepInstance& si : kInstances)
     if (si.consts(k) != cudaSuccess) { delete ctx; return GITM_ERR_CUDA; }
   // the scratch of gitm_vert_advance_native_noalloc on this device (a host-side
@@ -887,7 +890,7 @@ static int adjoint_prepare(GitmVertPlan* P) {
     P->adj_ready = true;
     return GITM_OK;
   }
-  const void* fn = adjoint_kernel_fn();
+  const void* fn = (plan_nalts(P) == 50) ? adjoint_kernel_fn_n50() : adjoint_kernel_fn();
   CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ctx->max_smem)));
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->adj_smem));
@@ -1011,7 +1014,7 @@ extern "C" int gitm_vert_plan_adjoint(GitmVertPlan* P, const GitmColumnAdjoint* 
   kp.saved = saved_states;
   kp.saved_ncols = P->n_cols_total;
   void* args[] = {&kp};
-  CUDA_TRY(ctx, cudaLaunchKernel(adjoint_kernel_fn(), dim3(P->adj_grid),
+  CUDA_TRY(ctx, cudaLaunchKernel((plan_nalts(P) == 50) ? adjoint_kernel_fn_n50() : adjoint_kernel_fn(), dim3(P->adj_grid),
                                  dim3(kAdjThreads), args, P->adj_smem, st));
   return GITM_OK;
 }

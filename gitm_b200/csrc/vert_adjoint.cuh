@@ -57,7 +57,9 @@ constexpr int SAVE_THREADS = 128;
 
 // Defined in vert_adjoint.cu (the kernel's own translation unit).
 const void* adjoint_kernel_fn();
+const void* adjoint_kernel_fn_n50();  // members of exactly 50 altitudes
 cudaError_t adjoint_set_consts(const Consts& k);
+cudaError_t adjoint_set_consts_n50(const Consts& k);
 __host__ __device__ inline int adj_state_doubles(int nAlts) { return NF * (nAlts + 4) + NPAS * NPC; }
 
 constexpr int ADJ_INLINE_BARS = 4;  // members whose descriptors travel in the kernel parameters
@@ -850,7 +852,10 @@ __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- the kernel
-template <int NT>
+// NA > 0: every member has exactly NA altitudes (the host checks), so the
+// layout offsets and loop bounds are compile-time constants; NA = 0 reads
+// nAlts from the member.
+template <int NT, int NA = 0>
 __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
@@ -868,7 +873,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
     const DevMember& M = kp.members[tile.member];
     const GitmColumnAdjoint B = (kp.n_inline > 0) ? kp.bars_inline[tile.member] : kp.bars[tile.member];
     const GitmColumnBatch& b = M.b;
-    const int nA = b.n_alts;
+    const int nA = (NA > 0) ? NA : b.n_alts;
     const int nc = tile.nc;
     const AdjLayout A = make_adj_layout(nA);
     const Layout& L = A.L;
