@@ -216,12 +216,13 @@ def opcount(n_alts: int, solver: str = "rusanov") -> float:
 
 
 def profile_traffic():
-    """DRAM bytes per column-step of the step kernel from the committed ncu
-    summary (profiles/vert_step_kernel_globe1deg.md), or None."""
+    """DRAM bytes per column and launch of the step kernel (the state is read
+    and written once per launch, whatever the steps per launch) from the
+    committed ncu summary (profiles/vert_step_kernel_globe1deg.md), or None."""
     p = os.path.join(ROOT, "profiles", "vert_step_kernel_globe1deg.md")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_column_step:\s*([0-9.eE+]+)", open(p).read())
+    m = re.search(r"dram_bytes_per_column_per_launch:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
 
 
@@ -505,7 +506,10 @@ def run_ours(args):
         traffic = profile_traffic() if args.solver == "rusanov" else None
         roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak,
-                "traffic": None if traffic is None else traffic * cs_launch,
+                "traffic": None if traffic is None else traffic * n_cols,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the "
+                                  "2 deg globe (profiles/vert_step_kernel_globe1deg.md), per column and "
+                                  "launch, times the columns of a launch",
                 "kernel": "vert_step_kernel",
                 "peak_source": "FP64 DGEMM (cuBLAS via torch.matmul 8192^3) measured in this run "
                                "(MEASURED_PEAKS.json has no FP64 figure)",
