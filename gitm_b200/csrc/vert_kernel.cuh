@@ -104,15 +104,16 @@ __device__ __forceinline__ bool in_pcells(int i, int nAlts) {
 
 __device__ __forceinline__ bool photochemical(int s) { return s == 3 || s == 4; }  // N(4S), NO
 
-// ModLimiter.f90:16-36, without branches: both candidates are formed and
-// the signs select one (the same values as the reference's if-blocks; lanes
-// whose cells take different cases do not split the warp)
+// ModLimiter.f90:16-36, without branches: on same-sign slopes the smallest
+// magnitude of beta u, beta d and (u + d) / 2 carries the common sign (the
+// reference's min of the three when both are positive and max when both are
+// negative, the same values since negation is exact); 0 otherwise.  Lanes
+// whose cells take different cases do not split the warp.
 __device__ __forceinline__ double limiter_mc(double u, double d, double beta) {
-  const double bu = beta * u, bd = beta * d, av = (u + d) * 0.5;
-  const double lo = fmin(fmin(bu, bd), av), hi = fmax(fmax(bu, bd), av);
+  const double m = fmin(fmin(fabs(beta * u), fabs(beta * d)), fabs((u + d) * 0.5));
   const bool pos = (u > 0.0) && (d > 0.0);
   const bool neg = !(u > 0.0) && (d < 0.0);
-  return pos ? lo : (neg ? hi : 0.0);
+  return pos ? m : (neg ? -m : 0.0);
 }
 
 struct ColCtx {
@@ -545,15 +546,18 @@ __device__ __forceinline__ void rusanov_cell(ColCtx c, int i, const GitmVertPara
   const double idc = c.g(GC_IDC, i);
   const double fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
   const double fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
+  // the halves taken once per cell: a product with 0.5 is exact, so
+  // d * (0.5 dF) and x * (0.5 / dAlt_C) round like (0.5 d) dF and (0.5 x) / dAlt_C
+  const double hF0 = 0.5 * dF0, hF1 = 0.5 * dF1, hidc = 0.5 * idc;
   // calc_rusanov_alts_rusanov (:694-718) at cell i
   auto sweep = [&](int f, double& grad, double& diff) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
     const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
-    const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
-    const double R0 = v[i] - 0.5 * d[i] * dF0;
-    const double L1 = v[i] + 0.5 * d[i] * dF1;
-    const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
-    grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+    const double L0 = fma(d[i - 1], hF0, v[i - 1]);
+    const double R0 = fma(-d[i], hF0, v[i]);
+    const double L1 = fma(d[i], hF1, v[i]);
+    const double R1 = fma(-d[i + 1], hF1, v[i + 1]);
+    grad = (L1 + R1 - L0 - R0) * hidc;
     diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
   };
   const double invr = c.g(GC_INVR, i), rr = c.g(GC_R, i), grav = c.g(GC_GRAV, i);
