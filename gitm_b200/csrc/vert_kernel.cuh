@@ -459,6 +459,11 @@ __device__ __forceinline__ void friction_solve(double dt, const double (&ns)[NS]
   double pw[NS];
 #pragma unroll
   for (int e = 0; e < NS; ++e) pw[e] = exp(c_k.one_minus_e[e] * lt);
+  // dt C_ij with dt taken into the densities once per cell: the entries
+  // -dt C_ij and the diagonal 1 + sum_j dt C_ij share each product
+  double nd[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) nd[q] = dt * ns[q];
   double a[NS][NS];
 #pragma unroll
   for (int r = 0; r < NS; ++r) {
@@ -466,11 +471,11 @@ __device__ __forceinline__ void friction_solve(double dt, const double (&ns)[NS]
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
       if (q == r) continue;
-      const double cij = c_k.kc[r][q] * ns[q] * pw[exp_index(r, q)];
-      a[r][q] = -dt * cij;
-      rs = rs + cij;
+      const double dcij = c_k.kc[r][q] * nd[q] * pw[exp_index(r, q)];
+      a[r][q] = -dcij;
+      rs = rs + dcij;
     }
-    a[r][r] = 1.0 + dt * rs;
+    a[r][r] = 1.0 + rs;
   }
   if (st) {
     bool diag_ok = true;
@@ -522,12 +527,15 @@ __device__ __forceinline__ void grad_log_cons(ColCtx c, int i, double (&glc)[NS]
     mc[q] = c.g(GC_M0 + q, i);
     lr5[q] = c.x(F_LRHO, i - 2 + q);
   }
+  // sum_q mc_q (log m_s + LogNS_s - LogRho) = sum_q mc_q (LogNS_s - LogRho) + log m_s sum_q mc_q:
+  // the species' constant leaves the five-point sum (one fma per point)
+  const double msum = ((mc[0] + mc[1]) + (mc[2] + mc[3])) + mc[4];
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     double acc = 0.0;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) acc += mc[q] * (c_k.log_mass[s] + c.x(F_LNS + s, i - 2 + q) - lr5[q]);
-    glc[s] = acc;
+    for (int q = 0; q < 5; ++q) acc = fma(mc[q], c.x(F_LNS + s, i - 2 + q) - lr5[q], acc);
+    glc[s] = fma(c_k.log_mass[s], msum, acc);
   }
 }
 
