@@ -453,12 +453,16 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
 // vertical_solver_rusanov.f90:694-718), forward and reverse.
 struct CellFaces {
   double dF0, dF1, idc, fc0, fc1;
+  double hF0, hF1, hidc;  // the halves of dF0, dF1, idc (a product with 0.5 is exact)
   double fc0b, fc1b;  // adjoints of the two dissipation coefficients
 
   __device__ __forceinline__ CellFaces(const ColCtx& c, int i) {
     dF0 = c.dAF(i);
     dF1 = c.dAF(i + 1);
     idc = c.g(GC_IDC, i);
+    hF0 = 0.5 * dF0;
+    hF1 = 0.5 * dF1;
+    hidc = 0.5 * idc;
     fc0 = 0.5 * fmax(c.cm(i - 1), c.cm(i));
     fc1 = 0.5 * fmax(c.cm(i), c.cm(i + 1));
     fc0b = 0.0;
@@ -467,11 +471,11 @@ struct CellFaces {
   __device__ __forceinline__ void sweep(const ColCtx& c, int f, int i, double& grad, double& diff) const {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
     const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
-    const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
-    const double R0 = v[i] - 0.5 * d[i] * dF0;
-    const double L1 = v[i] + 0.5 * d[i] * dF1;
-    const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
-    grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+    const double L0 = fma(d[i - 1], hF0, v[i - 1]);
+    const double R0 = fma(-d[i], hF0, v[i]);
+    const double L1 = fma(d[i], hF1, v[i]);
+    const double R1 = fma(-d[i + 1], hF1, v[i + 1]);
+    grad = (L1 + R1 - L0 - R0) * hidc;
     diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
   }
   // (gb, dbv) -> faces -> values and slopes; returns this cell's own share
@@ -480,20 +484,20 @@ struct CellFaces {
                                               double dbv) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
     const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
-    const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
-    const double R0 = v[i] - 0.5 * d[i] * dF0;
-    const double L1 = v[i] + 0.5 * d[i] * dF1;
-    const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
-    const double hg = 0.5 * idc * gb;
+    const double L0 = fma(d[i - 1], hF0, v[i - 1]);
+    const double R0 = fma(-d[i], hF0, v[i]);
+    const double L1 = fma(d[i], hF1, v[i]);
+    const double R1 = fma(-d[i + 1], hF1, v[i + 1]);
+    const double hg = hidc * gb;
     const double L1b = hg - fc1 * idc * dbv, R1b = hg + fc1 * idc * dbv;
     const double L0b = -hg + fc0 * idc * dbv, R0b = -hg - fc0 * idc * dbv;
     fc1b += idc * (R1 - L1) * dbv;
     fc0b += -idc * (R0 - L0) * dbv;
     a.add(f, i - 1, L0b);
-    a.dadd(f, i - 1, 0.5 * dF0 * L0b);
-    a.dadd(f, i, -0.5 * dF0 * R0b + 0.5 * dF1 * L1b);
+    a.dadd(f, i - 1, hF0 * L0b);
+    a.dadd(f, i, -hF0 * R0b + hF1 * L1b);
     a.add(f, i + 1, R1b);
-    a.dadd(f, i + 1, -0.5 * dF1 * R1b);
+    a.dadd(f, i + 1, -hF1 * R1b);
     return R0b + L1b;
   }
   // cMax through the dissipation coefficients (the branch of each max the

@@ -100,12 +100,14 @@ struct Faces {
 };
 __device__ __forceinline__ Faces kt_faces(ColCtx c, int f, int i, double vm, double v0, double vp) {
   const double* d = &c.col[c.L.DL + f * (c.L.nAlts + 2)];
-  const double dfm = c.dAF(i - 1), df0 = c.dAF(i), dfp = c.dAF(i + 1);
+  // halves of the cell widths: a product with 0.5 is exact, so d * (0.5 dF)
+  // rounds like (0.5 d) dF
+  const double hm = 0.5 * c.dAF(i - 1), h0 = 0.5 * c.dAF(i), hp = 0.5 * c.dAF(i + 1);
   Faces r;
-  r.lm = vm + 0.5 * d[i - 1] * dfm;
-  r.rm = v0 - 0.5 * d[i] * df0;
-  r.lp = v0 + 0.5 * d[i] * df0;
-  r.rp = vp - 0.5 * d[i + 1] * dfp;
+  r.lm = fma(d[i - 1], hm, vm);
+  r.rm = fma(-d[i], h0, v0);
+  r.lp = fma(d[i], h0, v0);
+  r.rp = fma(-d[i + 1], hp, vp);
   return r;
 }
 
@@ -114,12 +116,12 @@ __device__ __forceinline__ void ausm_sweep(ColCtx c, int fslope, int ffield, int
                                            double fc1, double& grad, double& diff) {
   const double* v = &c.col[c.xo + ffield * c.L.G + 1];
   const double* d = &c.col[c.L.DL + fslope * (c.L.nAlts + 2)];
-  const double dF0 = c.dAF(i), dF1 = c.dAF(i + 1), idc = c.g(GC_IDC, i);
-  const double L0 = v[i - 1] + 0.5 * d[i - 1] * dF0;
-  const double R0 = v[i] - 0.5 * d[i] * dF0;
-  const double L1 = v[i] + 0.5 * d[i] * dF1;
-  const double R1 = v[i + 1] - 0.5 * d[i + 1] * dF1;
-  grad = 0.5 * (L1 + R1 - L0 - R0) * idc;
+  const double hF0 = 0.5 * c.dAF(i), hF1 = 0.5 * c.dAF(i + 1), idc = c.g(GC_IDC, i);
+  const double L0 = fma(d[i - 1], hF0, v[i - 1]);
+  const double R0 = fma(-d[i], hF0, v[i]);
+  const double L1 = fma(d[i], hF1, v[i]);
+  const double R1 = fma(-d[i + 1], hF1, v[i + 1]);
+  grad = (L1 + R1 - L0 - R0) * (0.5 * idc);
   diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
 }
 
