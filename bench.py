@@ -446,7 +446,7 @@ def run_ours(args):
         t, spl, cps = (int(x) for x in args.launch.split(","))
         plan.set_config(threads=t, steps_per_launch=spl, ctas_per_sm=cps)
     elif not args.no_autotune:
-        plan.autotune(DT, min(args.steps, 8))
+        plan.autotune(DT, min(args.steps, 16))
     cfg = plan.config
     gs = GraphSteps(torch, plan, [dm], dev, args.steps)
     for _ in range(max(args.warmup, 1)):  # W untimed warm-up replays of the timed graphs

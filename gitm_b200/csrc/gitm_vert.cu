@@ -791,9 +791,13 @@ extern "C" int gitm_vert_plan_autotune(GitmVertPlan* P, double dt, int n_steps, 
   std::vector<std::pair<double*, double*>> bk;
   int rc = snapshot(P, bk, false);
   if (rc) return rc;
+  // steps per launch: one (the plain launch), n_steps and n_steps / 2
+  std::vector<int> spls{1};
+  if (n_steps / 2 > 1) spls.push_back(n_steps / 2);
+  if (n_steps > 1) spls.push_back(n_steps);
   std::vector<GitmLaunchConfig> cands;
   for (int t : kThreadChoices)
-    for (int spl : {1, n_steps})
+    for (int spl : spls)
       for (int cps : {0, 1, 2, 3}) {
         GitmLaunchConfig c{t, 0, spl, cps};
         cands.push_back(c);

@@ -243,7 +243,9 @@ int gitm_vert_plan_get_config(const GitmVertPlan* plan, GitmLaunchConfig* cfg);
 /* Runs n_steps RK4 steps of dt seconds (Dt in ModGITM) on every column.
  * Asynchronous; only kernel launches are issued, so it can be captured. */
 int gitm_vert_plan_advance(GitmVertPlan* plan, double dt, int n_steps, void* stream);
-/* Times candidate launch shapes on a scratch copy of the state and keeps the
+/* Times candidate launch shapes (every built CTA size, 1, n_steps / 2 and
+ * n_steps steps per launch, persistent grids of 0-3 CTAs per SM) over
+ * n_steps steps on a scratch copy of the state and keeps the
  * fastest; the plan's state is not modified.  Synchronous. */
 int gitm_vert_plan_autotune(GitmVertPlan* plan, double dt, int n_steps,
                             GitmLaunchConfig* chosen);
