@@ -130,9 +130,9 @@ struct SpeciesFaces {
   Faces rho, ps, hps, w;
 };
 __device__ __forceinline__ void species_faces(ColCtx c, int s, int i, double logk, bool with_p,
-                                              bool with_h, SpeciesFaces& o) {
+                                              bool with_h, SpeciesFaces& o, bool with_rho = true) {
   const double lm = c_k.log_mass[s];
-  {
+  if (with_rho) {
     const int f = AS_LRHOS + s;
     Faces t = kt_faces(c, f, i, c.x(F_LNS + s, i - 1), c.x(F_LNS + s, i), c.x(F_LNS + s, i + 1));
     o.rho.lm = exp(lm + t.lm);
@@ -265,10 +265,21 @@ __device__ __forceinline__ void ausm_cell(ColCtx c, int i, const GitmVertParams&
   double WLM = 0.0, WRM = 0.0, WLP = 0.0, WRP = 0.0;  // sums of RhoS * VertVel
   // one species at a time: the fully unrolled passes made a body the
   // instruction cache could not hold (2.76 -> 3.33 M column-steps/s)
+  // the density and pressure face states of each species, kept from this
+  // pass for the flux pass (per-thread memory, cached)
+  double fst[NS][8];
 #pragma unroll 1
   for (int s = 0; s < NS; ++s) {
     SpeciesFaces f;
     species_faces(c, s, i, logk, true, false, f);
+    fst[s][0] = f.rho.lm;
+    fst[s][1] = f.rho.rm;
+    fst[s][2] = f.rho.lp;
+    fst[s][3] = f.rho.rp;
+    fst[s][4] = f.ps.lm;
+    fst[s][5] = f.ps.rm;
+    fst[s][6] = f.ps.lp;
+    fst[s][7] = f.ps.rp;
     RhoLM = RhoLM + f.rho.lm;
     RhoRM = RhoRM + f.rho.rm;
     RhoLP = RhoLP + f.rho.lp;
@@ -317,7 +328,9 @@ __device__ __forceinline__ void ausm_cell(ColCtx c, int i, const GitmVertParams&
   for (int s = 0; s < NS; ++s) {
     const bool sh = (sub >> s) & 1u;
     SpeciesFaces f;
-    species_faces(c, s, i, logk, true, sh, f);
+    species_faces(c, s, i, logk, false, sh, f, false);
+    f.rho = Faces{fst[s][0], fst[s][1], fst[s][2], fst[s][3]};
+    f.ps = Faces{fst[s][4], fst[s][5], fst[s][6], fst[s][7]};
     double nvM, rfM, mfM, npM, nvP, rfP, mfP, npP;
     species_face_flux(f.rho.lm, f.rho.rm, f.ps.lm, f.ps.rm, f.hps.lm, f.hps.rm, f.w.lm, f.w.rm, CSM, kp, ku, dzdt,
                       sh, nvM, rfM, mfM, npM);
