@@ -187,6 +187,22 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
     // LogNS(0) on entry: NS(0) of line 93 is formed before the MSIS values
     // overwrite cell 0
     const double l0 = (s < NS) ? x(F_LNS + s, 0) : 0.0;
+    // the upper boundary's hydrostatic neutrals (lines 471-486, Temp(nA+1:nA+2)
+    // = Temp(nA)) read only interior cells: formed first, so that their
+    // division and exponentials overlap the lower boundary's work
+    double mu1 = 0.0, mu2 = 0.0;
+    if (s < NS) {
+      const double T = x(F_T, nA);
+      const double den = 0.5 * (T + T) * KB;
+      const double ish1 = (-0.5 * (sc[SC_EG + 3] + sc[SC_EG + 2])) * c_k.mass[s] / den;
+      const double ish2 = (-0.5 * (sc[SC_EG + 4] + sc[SC_EG + 3])) * c_k.mass[s] / den;
+      const double l1 = x(F_LNS + s, nA) - ish1 * sc[SC_DAF + 4];
+      const double l2 = l1 - ish2 * sc[SC_DAF + 5];
+      x(F_LNS + s, nA + 1) = l1;
+      x(F_LNS + s, nA + 2) = l2;
+      mu1 = c_k.mass[s] * exp(l1);
+      mu2 = c_k.mass[s] * exp(l2);
+    }
     __syncwarp();
     // lines 112-148
     if (msis) {
@@ -265,39 +281,38 @@ __device__ __forceinline__ void bc_column(ColCtx c, const GitmVertParams& prm, i
       c.ion(s, -1) = v;
     }
     __syncwarp();
-    // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1; with
-    // them the upper boundary's hydrostatic neutrals (lines 471-486,
-    // Temp(nA+1:nA+2) = Temp(nA)) and its LogRho (lines 598-604), which read
-    // only interior cells and these ghosts: the warp of the upper half keeps
-    // the ion chain alone, and the four LogRho ghosts share one log
+    // lines 348-362: LogRho and bulk vertical wind at cells 0 and -1, and
+    // the upper boundary's LogRho (lines 598-604) from the ghosts formed
+    // above: the warp of the upper half keeps the ion chain alone.  The six
+    // sums over species go through shared memory (the slope buffer is dead
+    // during the boundary passes; the upper half uses its first 63 doubles):
+    // lanes 0..3 add them in species order, one log serves the four cells
     {
-      double m0 = 0.0, m1 = 0.0, t0 = 0.0, t1 = 0.0, mu1 = 0.0, mu2 = 0.0;
+      double* sb = c.col + c.L.DL + 64;  // [6][NS]: m0, m1, t0, t1, mu1, mu2
       if (s < NS) {
-        const double T = x(F_T, nA);
-        const double den = 0.5 * (T + T) * KB;
-        const double ish1 = (-0.5 * (sc[SC_EG + 3] + sc[SC_EG + 2])) * c_k.mass[s] / den;
-        const double ish2 = (-0.5 * (sc[SC_EG + 4] + sc[SC_EG + 3])) * c_k.mass[s] / den;
-        const double l1 = x(F_LNS + s, nA) - ish1 * sc[SC_DAF + 4];
-        const double l2 = l1 - ish2 * sc[SC_DAF + 5];
-        x(F_LNS + s, nA + 1) = l1;
-        x(F_LNS + s, nA + 2) = l2;
-        m0 = c_k.mass[s] * exp(x(F_LNS + s, 0));
-        m1 = c_k.mass[s] * exp(x(F_LNS + s, -1));
-        mu1 = c_k.mass[s] * exp(l1);
-        mu2 = c_k.mass[s] * exp(l2);
-        t0 = m0 * x(F_W + s, 0);
-        t1 = m1 * x(F_W + s, -1);
+        const double m0 = c_k.mass[s] * exp(x(F_LNS + s, 0));
+        const double m1 = c_k.mass[s] * exp(x(F_LNS + s, -1));
+        sb[0 * NS + s] = m0;
+        sb[1 * NS + s] = m1;
+        sb[2 * NS + s] = m0 * x(F_W + s, 0);
+        sb[3 * NS + s] = m1 * x(F_W + s, -1);
+        sb[4 * NS + s] = mu1;
+        sb[5 * NS + s] = mu2;
       }
-      const double r0 = lane_seq_sum(m0, NS), r1 = lane_seq_sum(m1, NS);
-      const double v0 = lane_seq_sum(t0, NS), v1 = lane_seq_sum(t1, NS);
-      const double ru1 = lane_seq_sum(mu1, NS), ru2 = lane_seq_sum(mu2, NS);
-      // lanes 0..3 take cells 0, -1, nAlts+1, nAlts+2: one log for the four
-      // and one division for the two lower ones
+      __syncwarp();
+      // lanes 0..3 take cells 0, -1, nAlts+1, nAlts+2
       if (s < 4) {
-        const double r = (s == 0) ? r0 : (s == 1) ? r1 : (s == 2) ? ru1 : ru2;
+        const int q = (s < 2) ? s : s + 2;
+        double r = 0.0, v = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) r = r + sb[q * NS + k];
+        if (s < 2) {
+#pragma unroll
+          for (int k = 0; k < NS; ++k) v = v + sb[(2 + s) * NS + k];
+        }
         const int cell = (s < 2) ? -s : nA + s - 1;
         x(F_LRHO, cell) = log(r);
-        if (s < 2) x(F_VU, -s) = (s ? v1 : v0) / r;
+        if (s < 2) x(F_VU, -s) = v / r;
       }
     }
     // lines 364-376
