@@ -38,7 +38,7 @@ __device__ __forceinline__ int exp_index(int r, int q) {
 struct Layout {
   int nAlts, G;
   int nsl;  // slope fields in DL: 18 (Rusanov) or 32 (AUSM)
-  int X0, XP0, X1, XP1, O, OP, DL, TU, CM, GM, SC, LT, QS, stride;
+  int X0, XP0, X1, XP1, O, OP, OGH, DL, TU, CM, GM, SC, LT, QS, stride;
 };
 
 constexpr int NSLOPE_AUSM = 32;
@@ -72,6 +72,10 @@ __host__ __device__ inline Layout make_layout(int nAlts, int solver = GITM_SOLVE
   L.XP1 = o; o += NPAS * NPC;
   L.O = o;   o += orig_global ? 0 : NF * G;
   L.OP = o;  o += orig_global ? 0 : NPAS * NPC;
+  // orig_global: Orig's ghost cells (f * 4 + u, u over cells -1, 0,
+  // nAlts+1, nAlts+2) and passive-ion cells stay here as well, for the
+  // ghost reset after every stage
+  L.OGH = o; o += orig_global ? NF * 4 + NPAS * NPC : 0;
   L.DL = o;  o += L.nsl * (nAlts + 2);
   L.TU = o;  o += G;
   L.CM = o;  o += G;
@@ -969,7 +973,14 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           const int cl = w / per, r = w - cl * per;
           double* col = sm + size_t(L.stride) * cl;
           if constexpr (OG) {
-            ogb[size_t(cl) * operc + r] = col[xo + r];
+            const double v = col[xo + r];
+            ogb[size_t(cl) * operc + r] = v;
+            if (r >= NF * G) {
+              col[L.OGH + NF * 4 + (r - NF * G)] = v;
+            } else {
+              const int f = r / G, g = r - f * G;
+              if (g < 2 || g >= nA + 2) col[L.OGH + f * 4 + (g < 2 ? g : g - nA)] = v;
+            }
           } else {
             col[L.O + r] = col[xo + r];
           }
@@ -1064,13 +1075,12 @@ __global__ void __launch_bounds__(NT, MINB) vert_step_kernel(const KParams kp) {
           for (int w = tid; w < nc * per; w += NT) {
             const int cl = w / per, r = w - cl * per;
             double* col = sm + size_t(L.stride) * cl;
-            const double* ocol = OG ? ogb + size_t(cl) * operc : col + L.O;  // OP follows O in both
             if (r < NF * 4) {
               const int f = r >> 2, u = r & 3;
               const int g = (u < 2) ? u : nA + u;  // cells -1,0,nA+1,nA+2
-              col[nxo + f * G + g] = ocol[f * G + g];
+              col[nxo + f * G + g] = OG ? col[L.OGH + r] : col[L.O + f * G + g];
             } else {
-              col[nxpo + r - NF * 4] = ocol[NF * G + r - NF * 4];
+              col[nxpo + r - NF * 4] = OG ? col[L.OGH + r] : col[L.OP + r - NF * 4];
             }
           }
         }
