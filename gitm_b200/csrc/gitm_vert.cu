@@ -416,7 +416,7 @@ static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int
 
 static int build_tiles(GitmVertPlan* P) {
   GitmVertCtx* ctx = P->ctx;
-  if (!kernel_for(P->io, P->solver, P->cfg.threads))
+  if (!kernel_for(P->io, P->solver, P->cfg.threads, plan_nalts(P)))
     return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built for solver %d", P->cfg.threads, P->solver);
   P->tiles.clear();
   P->smem = 0;
