@@ -150,27 +150,68 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
   auto dAF = [&](int i) { return c.dAF(i); };
 
   if (part & 2) {
-    // lines 598-604: LogRho of the two top ghosts
-    for (int cc = nA + 1; cc <= nA + 2; ++cc) {
-      const double ms = (s < NS) ? c_k.mass[s] * exp(X(F_LNS + s, cc)) : 0.0;
-      const double r = lane_seq_sum(ms, NS);
-      const double lb = a.x(F_LRHO, cc);
+    // the pre-boundary ion ghosts (global memory) read first, so that their
+    // latency overlaps the LogRho pass
+    double pg1 = 0.0, pg2 = 0.0;
+    if (s < NI) {
+      pg1 = PI(s, nA + 1);
+      pg2 = PI(s, nA + 2);
+    }
+    // lines 598-604: LogRho of the two top ghosts (both cells' sums first)
+    {
+      double ms1 = 0.0, ms2 = 0.0;
+      if (s < NS) {
+        ms1 = c_k.mass[s] * exp(X(F_LNS + s, nA + 1));
+        ms2 = c_k.mass[s] * exp(X(F_LNS + s, nA + 2));
+      }
+      const double r1 = lane_seq_sum(ms1, NS);
+      const double r2 = lane_seq_sum(ms2, NS);
+      const double lb1 = a.x(F_LRHO, nA + 1), lb2 = a.x(F_LRHO, nA + 2);
       __syncwarp();
-      if (s < NS) a.x(F_LNS + s, cc) += lb * ms / r;
-      if (s == 0) a.x(F_LRHO, cc) = 0.0;
+      if (s < NS) {
+        a.x(F_LNS + s, nA + 1) += lb1 * ms1 / r1;
+        a.x(F_LNS + s, nA + 2) += lb2 * ms2 / r2;
+      }
+      if (s == 0) {
+        a.x(F_LRHO, nA + 1) = 0.0;
+        a.x(F_LRHO, nA + 2) = 0.0;
+      }
     }
     __syncwarp();
-    // lines 488-596: ions, one per lane
+    // lines 488-596: ions, one per lane.  With UseImprovedIonAdvection the
+    // logs of the extrapolation are taken lane-parallel first, as bc_column
+    // takes them: lg[7 s + j] = log(pre-boundary ion s at nAlts+2-j), j =
+    // 0..6; the ghost values the forward set (exp of its extrapolations) are
+    // read from the post-boundary state, and the log of the first one is its
+    // exponent y, as bc_column uses it.
     {
       const bool improved = prm.use_improved_ion_advection != 0;
       double tp = 0.0;
-      for (int i = 1 + lane; i <= nA; i += 32) tp += c.dAF(i) * (improved ? XI(0, i) : exp(XI(0, i)));
-      for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
-      const bool hold = (tp / 1e16 < prm.min_tec) && (sc[SC_PLASMA] != 0.0);
       bool neg = false;
-      if (improved && s < NI)
-        for (int q = nA - 5; q <= nA + 2; ++q) neg = neg || (((q >= nA + 1) ? PI(s, q) : XI(s, q)) < 0.0);
+      double* lg = c.col + c.L.DL;  // scratch: the slopes are dead during the boundary adjoint
+      static_assert(NI * 9 <= NSTENCIL * (8 + 2), "the ion logs and ghosts fit the slope region at nAlts >= 8");
+      if (improved) {
+        for (int i = 1 + lane; i <= nA; i += 32) tp += c.dAF(i) * XI(0, i);
+        if (s < NI) {
+          neg = (pg1 < 0.0) || (pg2 < 0.0);
+          for (int q = nA - 5; q <= nA; ++q) neg = neg || (XI(s, q) < 0.0);
+          lg[NI * 7 + s] = pg2;
+          lg[NI * 8 + s] = pg1;
+        }
+        __syncwarp();
+        for (int q = lane; q < NI * 7; q += 32) {
+          const int si = q / 7, j = q - si * 7;
+          const int cell = nA + 2 - j;
+          lg[q] = log((j < 2) ? lg[NI * (7 + j) + si] : XI(si, cell));
+        }
+      } else {
+        for (int i = 1 + lane; i <= nA; i += 32) tp += c.dAF(i) * exp(XI(0, i));
+      }
+      for (int off = 16; off > 0; off >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, off);
+      // the forward's test (bc_column): TEC < MinTEC * 1e16
+      const bool hold = (tp < prm.min_tec * 1e16) && (sc[SC_PLASMA] != 0.0);
       const bool anyneg = __any_sync(0xffffffffu, neg);
+      __syncwarp();
       const double dT = dAF(nA);
       if (anyneg) {
         if (lane == 0) atomicOr(st, GITM_ST_ADJ_BRANCH);
@@ -178,40 +219,36 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
         const double* C = bu;
         const double* D = bu + 5;
         if (improved) {
-          double n[6];
-          n[0] = log(PI(s, nA + 1));
-          for (int j = 1; j < 6; ++j) n[j] = log(XI(s, nA + 1 - j));
+          const double* n = lg + s * 7 + 1;  // n[k] = log(ion at nAlts+1-k), k = 0..5
+          const double g0 = lg[s * 7];
           const double dnr = C[0] * n[1] + C[1] * n[2] + C[2] * n[3] + C[3] * n[4] + C[4] * n[5];
           const double lim = -(0.001 * n[0] / dT);
           const bool t1 = dnr > lim;
           const double dn = t1 ? lim : dnr;
-          const double v1 = exp(n[1] + dn * dAF(nA + 1));
-          const double g0 = log(PI(s, nA + 2));
-          const double nn1 = log(v1);
-          const double dn2r = D[0] * nn1 + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
+          const double y = n[1] + dn * dAF(nA + 1);
+          const double v1 = XI(s, nA + 1);  // exp(y)
+          const double dn2r = D[0] * y + D[1] * n[1] + D[2] * n[2] + D[3] * n[3] + D[4] * n[4];
           const double lim2 = -(0.001 * g0 / dT);
           const bool t2 = dn2r > lim2;
-          const double dn2 = t2 ? lim2 : dn2r;
-          const double v2 = exp(nn1 + dn2 * dAF(nA + 2));
+          const double v2 = XI(s, nA + 2);  // exp(y + dn2 dAF(nAlts+2))
           double nb[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
           const double v2b = a.ion(s, nA + 2);
           a.ion(s, nA + 2) = 0.0;
           const double e2 = v2b * v2;
-          double nn1b = e2;
+          double yb = e2;
           const double dn2b = e2 * dAF(nA + 2);
           if (t2) {
-            a.ion(s, nA + 2) += (dn2b * (-0.001 / dT)) / PI(s, nA + 2);
+            a.ion(s, nA + 2) += (dn2b * (-0.001 / dT)) / pg2;
           } else {
-            nn1b += D[0] * dn2b;
+            yb += D[0] * dn2b;
             for (int q = 1; q < 5; ++q) nb[q] += D[q] * dn2b;
           }
-          const double v1b = a.ion(s, nA + 1) + nn1b / v1;
+          const double e1 = a.ion(s, nA + 1) * v1 + yb;
           a.ion(s, nA + 1) = 0.0;
-          const double e1 = v1b * v1;
           nb[1] += e1;
           const double dnb = e1 * dAF(nA + 1);
           if (t1) {
-            a.ion(s, nA + 1) += (dnb * (-0.001 / dT)) / PI(s, nA + 1);
+            a.ion(s, nA + 1) += (dnb * (-0.001 / dT)) / pg1;
           } else {
             for (int q = 0; q < 5; ++q) nb[q + 1] += C[q] * dnb;
           }
@@ -219,11 +256,11 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
         } else {
           const double dn1r = C[0] * XI(s, nA) + C[1] * XI(s, nA - 1) + C[2] * XI(s, nA - 2) +
                               C[3] * XI(s, nA - 3) + C[4] * XI(s, nA - 4);
-          const bool t1 = dn1r > -(0.001 * PI(s, nA + 1) / dT);
+          const bool t1 = dn1r > -(0.001 * pg1 / dT);
           const double v1 = XI(s, nA + 1);
           const double dn2r = D[0] * v1 + D[1] * XI(s, nA) + D[2] * XI(s, nA - 1) + D[3] * XI(s, nA - 2) +
                               D[4] * XI(s, nA - 3);
-          const bool t2 = dn2r > -(0.001 * PI(s, nA + 2) / dT);
+          const bool t2 = dn2r > -(0.001 * pg2 / dT);
           const double v2b = a.ion(s, nA + 2);
           a.ion(s, nA + 2) = 0.0;
           double v1b = a.ion(s, nA + 1) + v2b;
@@ -324,23 +361,36 @@ __device__ inline void bc_column_adjoint(const ColCtx& c, const ColAdj& a, const
       }
     }
     __syncwarp();
-    // lines 348-362: LogRho and bulk vertical wind of cells 0 and -1
-    for (int cc = 0; cc >= -1; --cc) {
-      const double we = (cc == 0) ? w0e : wm1e;
-      const double ms = (s < NS) ? c_k.mass[s] * exp(X(F_LNS + s, cc)) : 0.0;
-      const double r = lane_seq_sum(ms, NS);
-      const double mw = lane_seq_sum(ms * we, NS);
-      const double lrb = a.x(F_LRHO, cc), vub = a.x(F_VU, cc);
-      __syncwarp();
-      const double rb = lrb / r - vub * mw / (r * r);
-      const double mwb = vub / r;
+    // lines 348-362: LogRho and bulk vertical wind of cells 0 and -1 (both
+    // cells' sums first)
+    {
+      double ms0 = 0.0, msm = 0.0;
       if (s < NS) {
-        a.x(F_W + s, cc) += mwb * ms;
-        a.x(F_LNS + s, cc) += (rb + mwb * we) * ms;
+        ms0 = c_k.mass[s] * exp(X(F_LNS + s, 0));
+        msm = c_k.mass[s] * exp(X(F_LNS + s, -1));
+      }
+      const double r0 = lane_seq_sum(ms0, NS);
+      const double mw0 = lane_seq_sum(ms0 * w0e, NS);
+      const double rm = lane_seq_sum(msm, NS);
+      const double mwm = lane_seq_sum(msm * wm1e, NS);
+      const double lrb0 = a.x(F_LRHO, 0), vub0 = a.x(F_VU, 0);
+      const double lrbm = a.x(F_LRHO, -1), vubm = a.x(F_VU, -1);
+      __syncwarp();
+      const double rb0 = lrb0 / r0 - vub0 * mw0 / (r0 * r0);
+      const double mwb0 = vub0 / r0;
+      const double rbm = lrbm / rm - vubm * mwm / (rm * rm);
+      const double mwbm = vubm / rm;
+      if (s < NS) {
+        a.x(F_W + s, 0) += mwb0 * ms0;
+        a.x(F_LNS + s, 0) += (rb0 + mwb0 * w0e) * ms0;
+        a.x(F_W + s, -1) += mwbm * msm;
+        a.x(F_LNS + s, -1) += (rbm + mwbm * wm1e) * msm;
       }
       if (s == 0) {
-        a.x(F_LRHO, cc) = 0.0;
-        a.x(F_VU, cc) = 0.0;
+        a.x(F_LRHO, 0) = 0.0;
+        a.x(F_VU, 0) = 0.0;
+        a.x(F_LRHO, -1) = 0.0;
+        a.x(F_VU, -1) = 0.0;
       }
       __syncwarp();
     }
