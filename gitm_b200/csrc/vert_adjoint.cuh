@@ -14,8 +14,12 @@
 // the scatter back to the gather:
 //   scatter^T -> bc^T(X4) -> RK combination^T -> for k = 3..0:
 //     load X_k, recompute its slopes, stage_k^T at every interior cell
-//     (neighbour contributions by shared-memory atomics), slopes^T,
-//     bc^T(X_k) and the combination^T of X_k
+//     (one thread per cell writes its own cell's adjoint; the sweeps'
+//     shares of the neighbouring cells go by shuffles within a warp, through
+//     a small edge buffer across warps; GradLogConS's are left in shared
+//     memory), the gather of those shares (one thread per cell), slopes^T
+//     (one thread per field and run of cells), bc^T(X_k) and the
+//     combination^T of X_k
 //   -> bc^T(X0) -> gather^T and producers^T.
 // Shared memory per column: the state, its adjoint, the adjoint of Orig, the
 // slopes and their adjoints, the per-cell coefficients and their adjoints.
@@ -27,7 +31,7 @@ namespace gv {
 
 struct AdjLayout {
   Layout L;  // X0: the state; X1: its adjoint; O: the adjoint of Orig
-  int DB, CMB, GMB, TUB, MMB, LC, stride;
+  int DB, GU, CMB, GMB, TUB, MMB, LC, stride;
 };
 
 __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
@@ -36,6 +40,10 @@ __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
   const int G = nAlts + 4;
   int o = A.L.stride;
   A.DB = o;  o += NSTENCIL * (nAlts + 2);
+  // GradLogConS's -Eddy vb_s of interior cell i at [s * nAlts + i - 1], and
+  // their sum (for LogRho) at s = NS: cell_gather hands them to the
+  // neighbouring cells
+  A.GU = o;  o += (NS + 1) * nAlts;
   A.CMB = o; o += G;
   A.GMB = o; o += G;
   A.TUB = o; o += G;
@@ -45,15 +53,21 @@ __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
   return A;
 }
 
-__host__ __device__ inline size_t adj_smem_bytes(int nAlts, int nc) {
-  return size_t(make_adj_layout(nAlts).stride) * nc * sizeof(double) + size_t(nc) * 2 * sizeof(uint32_t);
-}
-
 constexpr int ADJ_NSTATE = 6;    // gathered state, X0, X1, X2, X3, X4
 // threads per CTA of the adjoint kernel (2 columns of 50 cells per CTA; 64
 // threads with one column measured 3 % slower) and of the saving step kernel
 constexpr int ADJ_THREADS = 128;
 constexpr int SAVE_THREADS = 128;
+// The stage adjoint's shares that cross a warp boundary inside a column: per
+// boundary (lane 31 of warp b | lane 0 of warp b+1) and swept field, the
+// value and slope shares to the right cell and to the left cell.
+constexpr int ADJ_EDGE_DOUBLES = (ADJ_THREADS / 32 - 1) * NSTENCIL * 4;
+
+// The columns' slots, the edge shares, then the status words.
+__host__ __device__ inline size_t adj_smem_bytes(int nAlts, int nc) {
+  return (size_t(make_adj_layout(nAlts).stride) * nc + ADJ_EDGE_DOUBLES) * sizeof(double) +
+         size_t(nc) * 2 * sizeof(uint32_t);
+}
 
 // Defined in vert_adjoint.cu (the kernel's own translation unit).
 const void* adjoint_kernel_fn();
@@ -100,6 +114,11 @@ __device__ __forceinline__ int limiter_mc_branch(double u, double d, double beta
   return pos ? cp : (neg ? cn : 0);
 }
 
+// Where a cell's neighbour is held in the stage adjoint: the next lane of
+// the same warp, a ghost cell (no thread; only this cell gives it shares
+// there), or a cell of the neighbouring warp.
+enum NbKind : int { NB_LANE = 0, NB_GHOST = 1, NB_WARP = 2 };
+
 // Per-column view of the adjoint arrays in shared memory.
 struct ColAdj {
   double* xb;    // adjoint of the state, [f*G + cell+1]
@@ -107,19 +126,42 @@ struct ColAdj {
   double* ob;    // adjoint of Orig
   double* obp;
   double* db;    // slope adjoints [f*(nAlts+2) + cell]
+  double* gu;    // GradLogConS's -Eddy vb_s [s*nAlts + i-1]; their sum at s = NS
   double* cmb;   // cMax adjoint [cell+1]
   double* gmb;   // Gamma adjoint
   double* tub;   // TempUnit adjoint
   double* mmb;   // MeanMajorMass(-1), MeanMajorMass(0), heating-factor sum
   uint8_t* lc;   // limiter branch of each slope [f*(nAlts+2) + cell] (limiter_mc_branch)
   int G, nA;
+  // the stage adjoint of interior cells (one thread per cell): the warp's
+  // lanes holding cells, where this cell's neighbours are, the CTA's edge
+  // shares and this thread's warp
+  unsigned mask;
+  int nbl, nbr;
+  double* eb;
+  int wid;
 
   __device__ __forceinline__ double& x(int f, int i) const { return xb[f * G + i + 1]; }
   __device__ __forceinline__ double& ion(int s, int i) const {
     return (s < NADV) ? xb[(F_I + s) * G + i + 1] : xbp[(s - NADV) * NPC + pcell(i, nA)];
   }
-  __device__ __forceinline__ void add(int f, int i, double v) const { atomicAdd(&xb[f * G + i + 1], v); }
-  __device__ __forceinline__ void dadd(int f, int c, double v) const { atomicAdd(&db[f * (nA + 2) + c], v); }
+  // In the stage adjoint the value and slope adjoints of interior cell i
+  // are written by its own thread alone (the neighbours' shares reach it by
+  // shuffles, or later through cell_gather), those of the ghost cells by
+  // the end cells' threads alone.
+  __device__ __forceinline__ void own(int f, int i, double v) const { xb[f * G + i + 1] += v; }
+  // a sweep's value share xv and slope share dv for neighbour cell j of kind
+  // nb (not NB_LANE); side 0: j = i+1, side 1: j = i-1
+  __device__ __forceinline__ void give(int f, int j, double xv, double dv, int nb, int side) const {
+    if (nb == NB_GHOST) {
+      own(f, j, xv);
+      db[f * (nA + 2) + j] += dv;
+    } else {
+      double* e = eb + ((wid - side) * NSTENCIL + f) * 4 + 2 * side;
+      e[0] += xv;
+      e[1] += dv;
+    }
+  }
 };
 
 // ---------------------------------------------------------------- boundaries^T
@@ -528,8 +570,10 @@ struct CellFaces {
     grad = (L1 + R1 - L0 - R0) * hidc;
     diff = (fc1 * (R1 - L1) - fc0 * (R0 - L0)) * idc;
   }
-  // (gb, dbv) -> faces -> values and slopes; returns this cell's own share
-  // of the value adjoint (the neighbours' shares go in by atomics)
+  // (gb, dbv) -> faces -> values and slopes; returns this cell's value
+  // share, with what the neighbouring cells of the same warp give it (by
+  // shuffles), and adds its slope share with theirs; the shares of ghost
+  // cells and of cells in the neighbouring warp go by give().
   __device__ __forceinline__ double sweep_adj(const ColCtx& c, const ColAdj& a, int f, int i, double gb,
                                               double dbv) {
     const double* v = &c.col[c.xo + f * c.L.G + 1];
@@ -543,12 +587,28 @@ struct CellFaces {
     const double L0b = -hg + fc0 * idc * dbv, R0b = -hg - fc0 * idc * dbv;
     fc1b += idc * (R1 - L1) * dbv;
     fc0b += -idc * (R0 - L0) * dbv;
-    a.add(f, i - 1, L0b);
-    a.dadd(f, i - 1, hF0 * L0b);
-    a.dadd(f, i, -hF0 * R0b + hF1 * L1b);
-    a.add(f, i + 1, R1b);
-    a.dadd(f, i + 1, -hF1 * R1b);
-    return R0b + L1b;
+    const double dl = hF0 * L0b;               // to the slope of cell i-1
+    const double dm = -hF0 * R0b + hF1 * L1b;  // this cell's slope
+    const double dr = -hF1 * R1b;              // the slope of cell i+1
+    const double xr = __shfl_down_sync(a.mask, L0b, 1);  // cell i+1's share of this cell
+    const double drr = __shfl_down_sync(a.mask, dl, 1);
+    const double xl = __shfl_up_sync(a.mask, R1b, 1);    // cell i-1's
+    const double dll = __shfl_up_sync(a.mask, dr, 1);
+    double own = R0b + L1b, down = dm;
+    if (a.nbl == NB_LANE) {
+      own += xl;
+      down += dll;
+    } else {
+      a.give(f, i - 1, L0b, dl, a.nbl, 1);
+    }
+    if (a.nbr == NB_LANE) {
+      own += xr;
+      down += drr;
+    } else {
+      a.give(f, i + 1, R1b, dr, a.nbr, 0);
+    }
+    a.db[f * (a.nA + 2) + i] += down;
+    return own;
   }
   // cMax through the dissipation coefficients (the branch of each max the
   // forward took)
@@ -600,7 +660,7 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
   for (int s = 0; s < NS; ++s) ns[s] = exp(c.x(F_LNS + s, i));
   const double ir = exp(-LR);
   // reverse of New LogRho = log(sumrho): the continuity adjoints, with
-  // New LogNS's own adjoint (read here, before the first shared atomic)
+  // New LogNS's own adjoint
   double nlb[NS];
   {
     const double srb = kb(F_LRHO) / sumrho;
@@ -673,18 +733,23 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
       vb[s] = inside ? wcb : 0.0;
       eddyb -= vb[s] * glc[s];
     }
-    // GradLogConS: 5-point mesh on log(m_s) + LogNS - LogRho
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      const double mc = c.g(GC_M0 + q, i);
-      double lrb = 0.0;
+    // GradLogConS: 5-point mesh on log(m_s) + LogNS - LogRho.  This
+    // cell's own share here; u_s = -Eddy vb_s (and their sum, for LogRho)
+    // left for cell_gather, which gives cells i-2, i-1, i+1, i+2 theirs
+    {
+      const double mc = c.g(GC_M0 + 2, i);
+      double lrb = 0.0, ul = 0.0;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        const double v = (-eddy * vb[s]) * mc;
+        const double u = -eddy * vb[s];
+        a.gu[s * a.nA + i - 1] = u;
+        ul += u;
+        const double v = u * mc;
         lrb -= v;
-        if (q == 2) lself[s] = v; else a.add(F_LNS + s, i - 2 + q, v);
+        lself[s] = v;
       }
-      if (q == 2) LRb += lrb; else a.add(F_LRHO, i - 2 + q, lrb);
+      a.gu[NS * a.nA + i - 1] = ul;
+      LRb += lrb;
     }
     // wb = M^-T vb with M = L U: U^T z = vb, then L^T wb = z
 #pragma unroll
@@ -732,7 +797,9 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
       irb += kvu * wc * m * ns[s];
       wb[s] = inside ? wcb : 0.0;
       lself[s] = 0.0;
+      a.gu[s * a.nA + i - 1] = 0.0;
     }
+    a.gu[NS * a.nA + i - 1] = 0.0;
   }
   // species momentum, continuity and their sweeps
   double gTb = 0.0, hzb = 0.0, corb = 0.0;
@@ -763,8 +830,8 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
     Lb += fa.sweep_adj(c, a, F_LNS + s, i, gLb, dLb);
     Wb += fa.sweep_adj(c, a, F_W + s, i, gWb, dWb);
     Lb += nsb[s] * ns[s];
-    a.add(F_LNS + s, i, Lb);
-    a.add(F_W + s, i, Wb);
+    a.own(F_LNS + s, i, Lb);
+    a.own(F_W + s, i, Wb);
   }
   LRb -= irb * ir;
   if (prm.use_coriolis) VEb += corb * dt * c.sc(SC_CORI);
@@ -773,10 +840,10 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
   // the species' share of the temperature sweep
   Tb += fa.sweep_adj(c, a, F_T, i, gTb, 0.0);
   fa.cmax_adj(c, a, i);
-  a.add(F_T, i, Tb);
-  a.add(F_VE, i, VEb);
-  a.add(F_VN, i, VNb);
-  a.add(F_LRHO, i, LRb);
+  a.own(F_T, i, Tb);
+  a.own(F_VE, i, VEb);
+  a.own(F_VN, i, VNb);
+  a.own(F_LRHO, i, LRb);
   return eddyb;
 }
 
@@ -785,7 +852,7 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
 __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i, double dt, double ivup,
                                          const double* kbp, int kstride) {
   auto kb = [&](int f) { return kbp[size_t(f) * kstride]; };
-  // the New adjoints this pass reads, before its first shared atomic
+  // the New adjoints this pass reads
   double ki[NADV];
 #pragma unroll
   for (int s = 0; s < NADV; ++s) ki[s] = kb(F_I + s);
@@ -805,7 +872,7 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
   for (int s = 0; s < NADV; ++s) {
     const double k = ki[s];
     const double own = fa.sweep_adj(c, a, F_I + s, i, -dt * ivup * k, dt * k);
-    a.add(F_I + s, i, k + own);
+    a.own(F_I + s, i, k + own);
   }
   // horizontal winds: New = V - dt VU gV + dt dV
   double VEb = kE + fa.sweep_adj(c, a, F_VE, i, -dt * VU * kE, dt * kE);
@@ -823,10 +890,10 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
   VUb += fa.sweep_adj(c, a, F_VU, i, divvb, 0.0);
   fa.cmax_adj(c, a, i);
   a.gmb[i + 1] += gmb;
-  a.add(F_T, i, Tb);
-  a.add(F_VE, i, VEb);
-  a.add(F_VN, i, VNb);
-  a.add(F_VU, i, VUb);
+  a.own(F_T, i, Tb);
+  a.own(F_VE, i, VEb);
+  a.own(F_VN, i, VNb);
+  a.own(F_VU, i, VUb);
 }
 
 // The limited slopes of cell i (interior: 4th-order form; cells 0 and
@@ -870,7 +937,11 @@ __device__ inline void slopes_adjoint_window(const ColCtx& c, const ColAdj& a, i
   const int nA = c.L.nAlts;
   const double* __restrict__ dbp = a.db + f * (nA + 2);
   const uint8_t* __restrict__ lcp = a.lc + f * (nA + 2);
+  // the state adjoint of field f (a region apart from the inputs: the loads
+  // of later cells may go ahead of the stores)
+  double* __restrict__ xo = a.xb + f * a.G + 1;
   double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0, w4 = 0.0;  // partial sums of cells i-2 .. i+2
+#pragma unroll 2
   for (int i = j0 - 2; i <= j1 + 2; ++i) {
     const bool ok = (i >= 0 && i <= nA + 1);  // slopes exist at cells 0..nAlts+1
     const int ic = min(max(i, 0), nA + 1);
@@ -887,12 +958,63 @@ __device__ inline void slopes_adjoint_window(const ColCtx& c, const ColAdj& a, i
     w2 += -cu * fa * ub + cd * fa * dbv;   // cell i
     w1 += cu * fb * ub - cd * fa * dbv;    // cell i-1
     w0 += cd * fb * dbv;                   // cell i-2: complete
-    if (i - 2 >= j0) a.x(f, i - 2) += w0;
+    if (i - 2 >= j0) xo[i - 2] += w0;
     w0 = w1;
     w1 = w2;
     w2 = w3;
     w3 = w4;
     w4 = 0.0;
+  }
+}
+
+// What reaches state cell m (-1..nAlts+2) of one column from the other
+// cells after the stage adjoint: GradLogConS's shares (u_s mc_q of interior
+// cell j = m - q + 2, q != 2, to LogNS_s; -sum_s u_s mc_q to LogRho) and,
+// when cell m and its neighbour sit on the two sides of a warp boundary,
+// the sweeps' shares the edge buffer holds.  One thread per cell: every
+// value and slope adjoint of the cell is written by that thread alone.
+// t0: the thread of the column's cell 1; nitems: threads holding cells.
+__device__ inline void cell_gather(const ColCtx& c, const ColAdj& a, int m, int t0, int nitems) {
+  const int nA = c.L.nAlts;
+  double mc[4];
+  int jj[4];
+  bool ok[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int d = (k < 2) ? k - 2 : k - 1;  // source cell m + d, d = -2, -1, 1, 2
+    const int j = m + d;
+    ok[k] = (j >= 1 && j <= nA);
+    jj[k] = ok[k] ? j : 1;
+    mc[k] = ok[k] ? c.g(GC_M0 + 2 - d, j) : 0.0;
+  }
+#pragma unroll
+  for (int s = 0; s <= NS; ++s) {
+    const double* u = a.gu + s * nA - 1;
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v += ok[k] ? u[jj[k]] * mc[k] : 0.0;
+    a.x((s < NS) ? F_LNS + s : F_LRHO, m) += (s < NS) ? v : -v;
+  }
+  // the edge shares (interior cells): t = this cell's thread
+  if (m >= 1 && m <= nA) {
+    const int t = t0 + m - 1;
+    const int lane = t & 31;
+    int bnd = -1, side = 0;
+    if (lane == 0 && m > 1) {
+      bnd = (t >> 5) - 1;  // the right cell of boundary bnd: what lane 31 gave it
+      side = 0;
+    } else if (lane == 31 && m < nA && t + 1 < nitems) {
+      bnd = t >> 5;  // the left cell: what lane 0 of the next warp gave it
+      side = 1;
+    }
+    if (bnd >= 0) {
+#pragma unroll 2
+      for (int f = 0; f < NSTENCIL; ++f) {
+        const double* e = a.eb + (bnd * NSTENCIL + f) * 4 + 2 * side;
+        a.x(f, m) += e[0];
+        a.db[f * (nA + 2) + m] += e[1];
+      }
+    }
   }
 }
 
@@ -911,6 +1033,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // nAlts from the member.
 template <int NT, int NA = 0>
 __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
+  static_assert(NT == ADJ_THREADS, "the edge-share buffer is sized for ADJ_THREADS");
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -934,12 +1057,18 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
     const int G = L.G;
     const int per = adj_state_doubles(nA);
     const int64_t ncols = b.n_cols;
-    uint32_t* sst = reinterpret_cast<uint32_t*>(sm + size_t(A.stride) * nc);
+    double* const eb = sm + size_t(A.stride) * nc;  // [ADJ_EDGE_DOUBLES]
+    uint32_t* sst = reinterpret_cast<uint32_t*>(eb + ADJ_EDGE_DOUBLES);
     uint32_t* sfrozen = sst + nc;
     const int nitems = nc * nA;
     const bool item = tid < nitems;
     const int my_cl = item ? tid / nA : 0;
     const int my_i = item ? tid % nA + 1 : 1;
+    // the stage adjoint's neighbours of this thread's cell (cells of a
+    // column are consecutive threads)
+    const unsigned imask = __ballot_sync(0xffffffffu, item);
+    const int nbl = (my_i == 1) ? NB_GHOST : (lane == 0) ? NB_WARP : NB_LANE;
+    const int nbr = (my_i == nA) ? NB_GHOST : (lane == 31) ? NB_WARP : NB_LANE;
     int cur = 0;
 
     auto ctx = [&](int cl) {
@@ -961,6 +1090,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       a.ob = col + L.O;
       a.obp = col + L.OP;
       a.db = col + A.DB;
+      a.gu = col + A.GU;
       a.cmb = col + A.CMB;
       a.gmb = col + A.GMB;
       a.tub = col + A.TUB;
@@ -968,6 +1098,11 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       a.lc = reinterpret_cast<uint8_t*>(col + A.LC);
       a.G = G;
       a.nA = nA;
+      a.mask = imask;
+      a.nbl = nbl;
+      a.nbr = nbr;
+      a.eb = eb;
+      a.wid = wid;
       return a;
     };
     auto gidx = [&](int f, int g, int cl) -> int64_t { return (int64_t(f) * G + g) * ncols + tile.c0 + cl; };
@@ -1289,6 +1424,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         double* db = sm + size_t(A.stride) * cl + A.DB;
         for (int r = tid; r < NSTENCIL * (nA + 2); r += NT) db[r] = 0.0;
       }
+      for (int r = tid; r < ADJ_EDGE_DOUBLES; r += NT) eb[r] = 0.0;
       __syncthreads();  // @phase 8
       for (int j = tid; j < nc * (nA + 2); j += NT) {
         const int cl = j / (nA + 2), i = j - cl * (nA + 2);
@@ -1300,13 +1436,16 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
         ColAdj a = adj(my_cl);
         eddy_bar += cell_adjoint_species(c, a, my_i, prm, dt, eddy, kbs, NT);
         cell_adjoint_rest(c, a, my_i, dt, ivup, kbs, NT);
-        // K = New - state: the state's own -K (K read into registers first:
-        // read between the shared atomics, each load would wait for the last)
-        double kv[NF];
+        // K = New - state: the state's own -K
 #pragma unroll
-        for (int f = 0; f < NF; ++f) kv[f] = kbs[size_t(f) * NT];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) a.add(f, my_i, -kv[f]);
+        for (int f = 0; f < NF; ++f) a.own(f, my_i, -kbs[size_t(f) * NT]);
+      }
+      __syncthreads();  // @phase 9
+      // GradLogConS's shares of the neighbouring cells and the sweeps'
+      // shares that crossed a warp boundary, one thread per cell
+      for (int w = tid; w < nc * G; w += NT) {
+        const int cl = w / G, m = w - cl * G - 1;
+        cell_gather(ctx(cl), adj(cl), m, cl * nA, nitems);
       }
       __syncthreads();  // @phase 9
       {
