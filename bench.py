@@ -836,8 +836,9 @@ def run_adjoint(args, fd_directions: int | None = None):
                                                       "CUDA events around each, mean of 10"},
                "timing": "median of 3 timed rollouts",
                "stages_kept": kept,
-               "backward_includes": "segment recompute (the step kernel saving its stage states) + one adjoint "
-                                    "kernel per step reading them",
+               "backward_includes": "segment recompute (the step kernel saving its stage states; the last "
+                                    "segment's were kept by the forward) + one adjoint kernel per step "
+                                    "reading them",
                "objective_value": Jv,
                "peak_memory": {"torch_allocated_bytes": int(peak_torch),
                                "device_used_delta_bytes": int(free0 - free1)},

@@ -13,7 +13,9 @@ sensitivity studies and data assimilation:
   ``n_steps`` rollout that keeps only every ``every``-th state in memory and
   recomputes the states of a segment when its adjoint runs (checkpointing);
   the recompute saves each step's stage states (``step_saving``) and the
-  adjoint kernel reads them.  ``every = 0`` keeps every step's input state
+  adjoint kernel reads them.  The last segment keeps its stage states from
+  the forward (the backward would recompute it first, into the same
+  buffers), so it is not recomputed.  ``every = 0`` keeps every step's input state
   and stage states from the forward itself (no recompute: about seven
   states of memory per step, ``stage_bytes_per_step``).
 * ``o_n2_objective`` is the column-weighted log(n_O / n_N2) at one altitude
@@ -77,9 +79,12 @@ class StepRunner:
         return torch.empty(self.plan.saved_state_doubles(), dtype=torch.float64,
                            device=self.dm.tensors["rho"].device)
 
-    def step_saving(self, state, saved, eddy=None, heating_scale=None) -> dict:
-        """step() that also writes the step's stage states to `saved`."""
-        self._load(state, eddy, heating_scale)
+    def step_saving(self, state, saved, eddy=None, heating_scale=None, loaded=False) -> dict:
+        """step() that also writes the step's stage states to `saved`.
+        loaded: the runner's arrays hold `state`, eddy and heating_scale
+        already (the output of the previous call), so nothing is copied in."""
+        if not loaded:
+            self._load(state, eddy, heating_scale)
         self.plan.advance_saving(self.dt, saved)
         return self.state()
 
@@ -165,8 +170,11 @@ class _Rollout(torch.autograd.Function):
                 raise V.GitmError(f"rollout with every = 0 keeps {need / 1e9:.1f} GB of stage states, "
                                   f"{free / 1e9:.1f} GB free: use checkpoints (every > 0)")
             s = {k: v.clone() for k, v in s.items()}
+        # with checkpoints, the last segment keeps its stage states from the
+        # forward (its recompute would be the first thing the backward does)
+        t_tail = 0 if every == 0 else ((n_steps - 1) // every) * every if n_steps > 0 else 0
         for t in range(n_steps):
-            if every == 0:
+            if t >= t_tail:
                 # keep the step's input and its stage states
                 buf = runner.saved_buffer()
                 stages.append((s, buf))
@@ -190,13 +198,16 @@ class _Rollout(torch.autograd.Function):
         hrun = runner.tensors.get("heating_scale")
         hb = None if hrun is None else torch.zeros_like(hrun)
         n, k = ctx.n_steps, ctx.every
-        if k == 0:
-            for j in reversed(range(n)):
-                st, buf = ctx.stages[j]
-                runner.vjp_into(st, y, eb, hb, eddy, hs, saved=buf)
-                ctx.stages[j] = None
-        else:
-            saved = []  # one stage-state buffer per step of a segment, reused
+        # the steps whose stages the forward kept (all of them with k = 0,
+        # else the last segment), then the checkpointed segments
+        saved = []  # one stage-state buffer per step of a segment, reused
+        for j in reversed(range(len(ctx.stages))):
+            st, buf = ctx.stages[j]
+            runner.vjp_into(st, y, eb, hb, eddy, hs, saved=buf)
+            ctx.stages[j] = None
+            if k > 0:
+                saved.insert(0, buf)
+        if k > 0:
             for seg in reversed(range(len(ctx.ckpts))):
                 t0 = seg * k
                 t1 = min(t0 + k, n)
@@ -205,7 +216,9 @@ class _Rollout(torch.autograd.Function):
                 while len(saved) < t1 - t0:
                     saved.append(runner.saved_buffer())
                 for j in range(t1 - t0):
-                    nxt = runner.step_saving(states[-1], saved[j], eddy, hs)
+                    # from the second step on, the runner's arrays hold the
+                    # step's input (the previous step's output) already
+                    nxt = runner.step_saving(states[-1], saved[j], eddy, hs, loaded=j > 0)
                     if j < t1 - t0 - 1:
                         states.append(nxt)
                 for j in reversed(range(t1 - t0)):

@@ -50,9 +50,14 @@ class LinearRunner:
     def saved_buffer(self):
         return torch.zeros(1, dtype=torch.float64)
 
-    def step_saving(self, state, saved, eddy=None, heating_scale=None):
+    def step_saving(self, state, saved, eddy=None, heating_scale=None, loaded=False):
         self.saved_calls += 1
         saved.fill_(1.0)  # marks the buffer as written by a saving step
+        if loaded:
+            # the caller says the arrays hold the step's input already
+            for k in AD.STATE:
+                assert torch.equal(self.tensors[k], state[k]), k
+            state, eddy, heating_scale = self.state(), None, None
         return self.step(state, eddy, heating_scale)
 
     def stage_bytes_per_step(self):
@@ -94,7 +99,7 @@ def _reference_grads(run, n):
 
 
 def test_rollout_modes_match_autograd():
-    for n, every in [(7, 0), (7, 1), (7, 3), (6, 3), (5, 10)]:
+    for n, every in [(7, 0), (7, 1), (7, 3), (6, 3), (5, 10), (10, 5), (1, 3)]:
         run = LinearRunner()
         want = _reference_grads(run, n)
         s0 = {k: run.tensors[k].clone().requires_grad_(True) for k in AD.STATE}
@@ -105,5 +110,6 @@ def test_rollout_modes_match_autograd():
         for name, g, w in zip(list(AD.STATE) + ["eddy", "heating_scale"], got, want):
             assert torch.allclose(g, w, rtol=1e-12, atol=1e-14), (n, every, name)
         # kept stages: one saving step per step in the forward, none after;
-        # checkpoints: one saving step per step in the backward
+        # checkpoints: one saving step per step, the last segment's in the
+        # forward, the others' in the backward
         assert run.saved_calls == n, (n, every, run.saved_calls)
