@@ -679,7 +679,7 @@ __device__ __forceinline__ void rusanov_slopes_cell(ColCtx c, int i, double beta
   // lets the loads of later fields be issued ahead of earlier stores
   const double* __restrict__ xv = c.col + c.xo + 1;
   double* __restrict__ sl = c.col + c.L.DL + i;
-#pragma unroll 3
+#pragma unroll 9
   for (int f = 0; f < NSTENCIL; ++f) {
     const double* v = xv + f * c.L.G;
     const double u = cu * (a * (v[i + 1] - v[i]) - b * (v[ip2] - v[i - 1]));
