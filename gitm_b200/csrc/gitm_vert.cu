@@ -238,23 +238,29 @@ static void grid_coefs(int nA, const double* alt, const double* grav, const doub
 // three CTAs share an SM and overlap each other's barrier phases.
 // The 512-thread shape also keeps Orig in its scratch slot (orig_global):
 // 8 columns of 50 altitudes then fit the shared memory of an SM, 16 warps at
-// 128 registers.
-struct Shape { int threads, min_blocks; bool acc_global, orig_global; };
-static const Shape kShapes[] = {{128, 3, true, false}, {160, 2, true, false}, {192, 2, true, false},
-                                {256, 1, false, false}, {320, 1, false, false}, {384, 1, false, false},
-                                {512, 1, true, true}};
+// 128 registers.  The AUSM solver's 384-thread shape does the same (6
+// columns of its larger slot instead of 4).  solver -1: any solver.
+struct Shape { int threads, solver, min_blocks; bool acc_global, orig_global; };
+static const Shape kShapes[] = {{128, -1, 3, true, false}, {160, -1, 2, true, false}, {192, -1, 2, true, false},
+                                {256, -1, 1, false, false}, {320, -1, 1, false, false},
+                                {384, GITM_SOLVER_AUSM, 1, true, true}, {384, -1, 1, false, false},
+                                {512, -1, 1, true, true}};
 static const int kThreadChoices[] = {128, 160, 192, 256, 320, 384, 512};
 
-static bool acc_global(int threads) {
+static const Shape* shape_of(int threads, int solver) {
   for (const Shape& s : kShapes)
-    if (s.threads == threads) return s.acc_global;
-  return false;
+    if (s.threads == threads && (s.solver == solver || s.solver < 0)) return &s;
+  return nullptr;
 }
 
-static bool orig_global(int threads) {
-  for (const Shape& s : kShapes)
-    if (s.threads == threads) return s.orig_global;
-  return false;
+static bool acc_global(int threads, int solver) {
+  const Shape* s = shape_of(threads, solver);
+  return s && s->acc_global;
+}
+
+static bool orig_global(int threads, int solver) {
+  const Shape* s = shape_of(threads, solver);
+  return s && s->orig_global;
 }
 
 // The step kernels, each compiled in its own translation unit
@@ -410,7 +416,7 @@ static int cols_per_cta(const GitmVertCtx* ctx, const GitmLaunchConfig& cfg, int
   int nc = cfg.cols_per_cta > 0 ? cfg.cols_per_cta : cfg.threads / nA;
   nc = std::min(nc, cfg.threads / 32);  // one BC warp per column
   nc = std::min(nc, cfg.threads / nA);  // every interior cell has a thread
-  while (nc > 1 && smem_bytes(nA, nc, solver, orig_global(cfg.threads)) > ctx->max_smem) --nc;
+  while (nc > 1 && smem_bytes(nA, nc, solver, orig_global(cfg.threads, solver)) > ctx->max_smem) --nc;
   return std::max(nc, 1);
 }
 
@@ -420,7 +426,7 @@ static int build_tiles(GitmVertPlan* P) {
     return set_err(ctx, GITM_ERR_ARG, "threads per CTA %d not built for solver %d", P->cfg.threads, P->solver);
   P->tiles.clear();
   P->smem = 0;
-  const bool og = orig_global(P->cfg.threads);
+  const bool og = orig_global(P->cfg.threads, P->solver);
   size_t orig_per_cta = 0;  // doubles of Orig a CTA's scratch slot holds (orig_global shapes)
   for (int m = 0; m < P->n_members; ++m) {
     const GitmColumnBatch& b = P->host_members[m];
@@ -450,7 +456,7 @@ static int build_tiles(GitmVertPlan* P) {
   const int T = P->cfg.threads;
   int grid = int(P->tiles.size());
   int per_sm = P->cfg.ctas_per_sm;
-  if (acc_global(T) && per_sm <= 0) {
+  if (acc_global(T, P->solver) && per_sm <= 0) {
     const void* fn = kernel_for(P->io, P->solver, T, plan_nalts(P));
     CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, P->smem));
     per_sm = std::max(per_sm, 1);
@@ -458,7 +464,7 @@ static int build_tiles(GitmVertPlan* P) {
   if (per_sm > 0) grid = std::min(grid, per_sm * ctx->num_sms);
   P->grid = std::max(grid, 1);
   P->scratch_per_cta = int64_t(NF) * T + int64_t(orig_per_cta);
-  if (acc_global(T)) {
+  if (acc_global(T, P->solver)) {
     // at least three slots: the host-pointer path splits them over 3 streams
     const size_t need = size_t(std::max(P->grid, 3)) * size_t(P->scratch_per_cta);
     if (need > P->scratch_doubles) {

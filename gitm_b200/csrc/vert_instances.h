@@ -47,7 +47,8 @@
   X(ausm0_t256_n50, 0, 256, 1, false, 1, false, 50, false)    \
   X(rus0_t128_save_n50, 0, 128, 3, true, 0, true, 50, false)  \
   X(rus0_t512_og, 0, 512, 1, true, 0, false, 0, true)         \
-  X(rus0_t512_og_n50, 0, 512, 1, true, 0, false, 50, true)
+  X(rus0_t512_og_n50, 0, 512, 1, true, 0, false, 50, true)    \
+  X(ausm0_t384_og_n50, 0, 384, 1, true, 1, false, 50, true)
 
 namespace gv {
 #define GV_DECLARE_INSTANCE(id, IO, NT, MINB, ACC, SOLVER, SAVE, NA, OG) \

@@ -36,7 +36,8 @@ VARIANTS = {
 }
 
 
-@pytest.mark.parametrize("threads", [128, 256])
+# 384 threads: the shape with Orig in global scratch, built for nAlts = 50
+@pytest.mark.parametrize("threads", [128, 256, 384])
 @pytest.mark.parametrize("variant", list(VARIANTS))
 def test_ausm_step_matches_oracle(torch_cuda, oracle_lib, variant, threads):
     p = ausm(**VARIANTS[variant])
@@ -64,13 +65,14 @@ def test_ausm_other_altitude_counts(torch_cuda, oracle_lib, n_alts):
     assert_state_close(out, ref, STATE)
 
 
-def test_ausm_multistep_resident(torch_cuda, oracle_lib):
+@pytest.mark.parametrize("threads", [256, 384])
+def test_ausm_multistep_resident(torch_cuda, oracle_lib, threads):
     p = ausm()
     m = synthetic.make_member(48, 50, seed=44)
     ref, _ = ref_advance(oracle_lib, m, p, 2.0, n_steps=5)
-    out, _ = gpu_advance(m, p, 2.0, n_steps=5, config=dict(steps_per_launch=5))
+    out, _ = gpu_advance(m, p, 2.0, n_steps=5, config=dict(threads=threads, steps_per_launch=5))
     assert_state_close(out, ref, STATE, rtol=1e-9)
-    out1, _ = gpu_advance(m, p, 2.0, n_steps=5, config=dict(steps_per_launch=1))
+    out1, _ = gpu_advance(m, p, 2.0, n_steps=5, config=dict(threads=threads, steps_per_launch=1))
     assert_state_close(out, out1, STATE, rtol=1e-12)
 
 
@@ -139,5 +141,5 @@ def test_ausm_autotune(torch_cuda):
     dm = V.device_member(m)
     plan = V.Plan(ctx, [dm])
     cfg = plan.autotune(2.0, 2)
-    assert cfg.threads in (128, 256)
+    assert cfg.threads in (128, 256, 384)
     np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
