@@ -113,6 +113,25 @@ def test_adjoint_matches_autograd(cuda, variant):
         assert _rel(g, w) < 1e-9, (k, _rel(g, w))
 
 
+@pytest.mark.parametrize("n_alts", [8, 30, 75, 128])
+def test_adjoint_other_altitude_counts(cuda, n_alts):
+    """The adjoint kernel built for any nAlts: several columns per CTA
+    (8, 30), one (75, 128), warp boundaries inside a column at different
+    cells, against autograd through the transcription."""
+    p = abi.default_params()
+    m = synthetic.make_member(12, n_alts, seed=80 + n_alts, with_heating=True)
+    gen = torch.Generator().manual_seed(6)
+    y = _ybar(m, gen, cuda)
+    want = _torch_vjp(m, p, 2.0, y, cuda)
+    got, status = _gpu_vjp(m, p, 2.0, y)
+    assert status == (0, 0)
+    for k, w in want.items():
+        g = got[k]
+        if k == "idensity_s":
+            g, w = g[:9], w[:9]
+        assert _rel(g, w) < 1e-9, (n_alts, k, _rel(g, w))
+
+
 @pytest.mark.parametrize("every", [2, 0])
 def test_rollout_equals_stepwise_composition(cuda, every):
     """Checkpoints every 2 steps, and every step's stages kept (every = 0)."""
