@@ -446,7 +446,9 @@ def run_ours(args):
         t, spl, cps = (int(x) for x in args.launch.split(","))
         plan.set_config(threads=t, steps_per_launch=spl, ctas_per_sm=cps)
     elif not args.no_autotune:
-        plan.autotune(DT, min(args.steps, 16))
+        # tuned on the timed step count itself when it is short (its steps
+        # per launch then divide it: 1, K/2 or K), else on 16 steps
+        plan.autotune(DT, args.steps if args.steps <= 32 else 16)
     cfg = plan.config
     gs = GraphSteps(torch, plan, [dm], dev, args.steps)
     for _ in range(max(args.warmup, 1)):  # W untimed warm-up replays of the timed graphs
