@@ -570,13 +570,8 @@ def e2e_leg(torch, V, ctx, m, n_steps: int, world: int, dev, optional_outputs: b
     ins = ("ndensity_s", "idensity_s", "rho", "temperature", "velocity", "vert_vel", "ivel_up", "eddy",
            "cos_lat", "sza", "mlat")
     outs = STATE_NAMES + (("log_ns", "ndensity") if optional_outputs else ())
-    from gitm_b200 import abi
     h2d = sum(getattr(pinned, k).nbytes for k in ins)
     d2h = sum(getattr(pinned, k).nbytes for k in outs)
-    # the passive ions change only at their 11 boundary cells: their other
-    # rows are not copied back
-    n_passive = abi.NIONS - 1 - abi.NIONS_ADVECT
-    d2h -= n_passive * (m.n_alts + 4 - 11) * m.n_cols * 8
     V.advance_vertical_all_host(ctx, [pinned], DT, 1)
     if world > 1:
         dist.barrier()
@@ -593,8 +588,7 @@ def e2e_leg(torch, V, ctx, m, n_steps: int, world: int, dev, optional_outputs: b
     return {"value": m.n_cols * n_steps * world / ee, "unit": UNIT,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "how": "gitm_vert_advance_native_host per step: the pinned host arrays advance_vertical "
-                   "reads copied in, stepped, the state it writes copied out (the passive ions' rows "
-                   "only at their boundary cells, where the step changes them)"
+                   "reads copied in, stepped, the state it writes copied out"
                    + (" with the optional LogNS and NDensity outputs" if optional_outputs else "")
                    + " (16 chunks, copies in / steps / copies out on three streams); wall clock"}
 

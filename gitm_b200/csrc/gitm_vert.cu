@@ -1288,29 +1288,9 @@ extern "C" int gitm_vert_advance_native_host(GitmVertCtx* ctx, const GitmColumnB
                                         a.field == &GitmColumnBatch::temp_unit || a.field == &GitmColumnBatch::cmax))
         continue;
       if (!prm.compute_eddy && a.field == &GitmColumnBatch::eddy) continue;
-      // row runs [r0, r1) to copy back: all rows, except that the passive
-      // ions change only at their boundary cells (-1, 0, 1, nAlts-5 ..
-      // nAlts+2; the step writes nothing else of them), so their other rows
-      // hold what was copied in and are not copied back
-      std::vector<std::pair<int64_t, int64_t>> runs;
-      if (a.field == &GitmColumnBatch::idensity_s) {
-        runs.push_back({0, int64_t(NADV) * G});  // advected ions
-        for (int q = NADV; q < NI; ++q) {
-          runs.push_back({int64_t(q) * G, int64_t(q) * G + 3});
-          runs.push_back({int64_t(q) * G + b.n_alts - 4, int64_t(q + 1) * G});
-        }
-        runs.push_back({int64_t(NI) * G, int64_t(NI + 1) * G});  // electrons
-      } else {
-        runs.push_back({0, rows_of(a.rows_per_cell, G)});
-      }
-      for (const auto& r : runs) {
-        cudaError_t e = cudaMemcpy2DAsync(b.*(a.field) + r.first * b.n_cols + ch.c0, hp, d.*(a.field) + r.first * ch.n,
-                                          w, w, r.second - r.first, cudaMemcpyDeviceToHost, s_out);
-        if (e != cudaSuccess) {
-          rc = set_err(ctx, GITM_ERR_CUDA, "copy back: %s", cudaGetErrorString(e));
-          break;
-        }
-      }
+      cudaError_t e = cudaMemcpy2DAsync(b.*(a.field) + ch.c0, hp, d.*(a.field), w, w,
+                                        rows_of(a.rows_per_cell, G), cudaMemcpyDeviceToHost, s_out);
+      if (e != cudaSuccess) rc = set_err(ctx, GITM_ERR_CUDA, "copy back: %s", cudaGetErrorString(e));
     }
   }
   for (cudaStream_t st : ctx->streams) cudaStreamSynchronize(st);

@@ -228,6 +228,28 @@ def test_host_pointer_path_matches_oracle(torch_cuda, oracle_lib):
         np.testing.assert_array_equal(getattr(h, k), dev_out[k], err_msg=k)
 
 
+def test_host_pointer_path_floors_passive_ions(torch_cuda, oracle_lib):
+    """With UseImprovedIonAdvection the step floors every ion density of the
+    interior cells at 1, the passive ions' too: the host form must bring
+    those interior values back as well (against the oracle)."""
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    m = synthetic.make_member(300, 50, seed=29)
+    rng = np.random.default_rng(3)
+    for q in range(abi.NIONS_ADVECT, abi.NIONS - 1):
+        cols = rng.choice(m.n_cols, 20, replace=False)
+        cells = rng.integers(4, 40, 20)  # interior cells away from the boundary rows
+        m.idensity_s[q, cells + 1, cols] = 0.5
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0)
+    h = m.copy()
+    ctx = V.VerticalContext(p)
+    V.advance_vertical_all_host(ctx, [h], 2.0)
+    ctx.close()
+    assert (st_ref == 0).all()
+    assert (ref["idensity_s"][abi.NIONS_ADVECT:abi.NIONS - 1, 2:51] >= 1.0).all()
+    assert_state_close(dict(h.arrays()), ref, STATE)
+
+
 def test_globe5deg_100_steps_each_against_the_oracle(torch_cuda, oracle_lib):
     """The 5 deg globe (36 x 72 = 2,592 columns, GITM's 4 x 8 blocks of 9 x 9),
     nAlts = 50, 100 RK4 steps of dt = 2 s through the plain per-call drop-in
