@@ -83,3 +83,69 @@ def test_transcription_gradient_matches_finite_differences():
         assert abs(fd - ana) <= 1e-6 * max(abs(fd), abs(ana)) + noise, (trial, fd, ana)
         checked += 1
     assert checked >= 4
+
+
+def test_rollout_finite_differences_track_branch_flips():
+    """A six-step rollout of the objective's form, central differences for
+    eps from 1e-6 to 1e-9 (relative) in random directions.  The MC limiter
+    makes the step piecewise smooth: a perturbation can flip a limiter case
+    (or a clamp, a boundary switch) somewhere in the rollout, and then the
+    difference quotient mixes two pieces.  Checked: wherever the +-eps runs
+    take exactly the base run's branches (the transcription's recorder), the
+    difference agrees with the autograd gradient to 1e-6 (beyond a rounding
+    floor of the difference of two J); every disagreement beyond 1e-6 comes
+    with flipped branches; some directions flip branches at the larger eps."""
+    p = abi.default_params()
+    m = synthetic.make_member(4, 20, seed=7, with_heating=True)
+    st, inp = TS.from_member(m, requires_grad=True)
+    names = ("nd", "temp", "vel", "ww", "rho")
+    w = torch.rand(4, dtype=torch.float64, generator=torch.Generator().manual_seed(1))
+    n_steps = 6
+
+    def J(state):
+        s = state
+        for _ in range(n_steps):
+            out = TS.step(s, inp, p, 2.0)
+            s = {k: out[k] for k in ("nd", "ion", "rho", "temp", "vel", "ww")}
+        return _objective(out, w)
+
+    def J_and_branches(state):
+        box = {}
+
+        def run():
+            box["j"] = float(J(state))
+        sig = TS.branch_signature(run)
+        return box["j"], sig
+
+    j = J(st)
+    grads = torch.autograd.grad(j, [st[n] for n in names])
+    base = {k: v.detach() for k, v in st.items()}
+    j0, sig0 = J_and_branches(base)
+    rng = np.random.default_rng(2)
+    dirs = [[torch.from_numpy(rng.normal(size=base[n].shape)) for n in names] for _ in range(6)]
+    checked = flipped = 0
+    for eps in (1e-6, 1e-7, 1e-8, 1e-9):
+        for d in dirs:
+            steps = [base[n].abs() * eps for n in names]
+
+            def point(sign):
+                s2 = dict(base)
+                for n, dd, ss in zip(names, d, steps):
+                    s2[n] = base[n] + sign * dd * ss
+                return s2
+            jp, sp = J_and_branches(point(1.0))
+            jm, sm = J_and_branches(point(-1.0))
+            fd = (jp - jm) / 2.0
+            ana = sum(float((g * dd * ss).sum()) for g, dd, ss in zip(grads, d, steps))
+            err = abs(fd - ana)
+            tol = 1e-6 * max(abs(fd), abs(ana)) + 3e-14 * abs(j0)
+            same = TS.same_branches(sig0, sp) and TS.same_branches(sig0, sm)
+            if same:
+                assert err <= tol, (eps, fd, ana)
+                checked += 1
+            else:
+                flipped += 1
+            # a disagreement beyond the tolerance only with flipped branches
+            assert err <= tol or not same, (eps, fd, ana)
+    assert checked >= 6
+    assert flipped >= 1
