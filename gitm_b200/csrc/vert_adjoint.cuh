@@ -31,7 +31,7 @@ namespace gv {
 
 struct AdjLayout {
   Layout L;  // X0: the state; X1: its adjoint; O: the adjoint of Orig
-  int DB, GU, CMB, GMB, TUB, MMB, LC, stride;
+  int DB, GU, FB, CMB, GMB, TUB, MMB, LC, stride;
 };
 
 __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
@@ -44,6 +44,9 @@ __host__ __device__ inline AdjLayout make_adj_layout(int nAlts) {
   // their sum (for LogRho) at s = NS: cell_gather hands them to the
   // neighbouring cells
   A.GU = o;  o += (NS + 1) * nAlts;
+  // the dissipation coefficients' adjoints of interior cell i (halved): its
+  // lower face at [i - 1], its upper face at [nAlts + i - 1]
+  A.FB = o;  o += 2 * nAlts;
   A.CMB = o; o += G;
   A.GMB = o; o += G;
   A.TUB = o; o += G;
@@ -127,6 +130,7 @@ struct ColAdj {
   double* obp;
   double* db;    // slope adjoints [f*(nAlts+2) + cell]
   double* gu;    // GradLogConS's -Eddy vb_s [s*nAlts + i-1]; their sum at s = NS
+  double* fb;    // the dissipation coefficients' adjoints, halved [i-1], [nAlts + i-1]
   double* cmb;   // cMax adjoint [cell+1]
   double* gmb;   // Gamma adjoint
   double* tub;   // TempUnit adjoint
@@ -610,12 +614,14 @@ struct CellFaces {
     a.db[f * (a.nA + 2) + i] += down;
     return own;
   }
-  // cMax through the dissipation coefficients (the branch of each max the
-  // forward took)
-  __device__ __forceinline__ void cmax_adj(const ColCtx& c, const ColAdj& a, int i) const {
-    const double cmm = c.cm(i - 1), cm0 = c.cm(i), cmp = c.cm(i + 1);
-    if (cmm >= cm0) atomicAdd(&a.cmb[i], 0.5 * fc0b); else atomicAdd(&a.cmb[i + 1], 0.5 * fc0b);
-    if (cm0 >= cmp) atomicAdd(&a.cmb[i + 1], 0.5 * fc1b); else atomicAdd(&a.cmb[i + 2], 0.5 * fc1b);
+  // the dissipation coefficients' adjoints (fc = 0.5 max(cMax, cMax') at
+  // each face), kept for cell_gather, which hands them to the cMax of the
+  // side each max took; acc: add to what the cell's other pass kept
+  __device__ __forceinline__ void keep_fc(const ColAdj& a, int i, bool acc) const {
+    double& b0 = a.fb[i - 1];
+    double& b1 = a.fb[a.nA + i - 1];
+    b0 = acc ? b0 + 0.5 * fc0b : 0.5 * fc0b;
+    b1 = acc ? b1 + 0.5 * fc1b : 0.5 * fc1b;
   }
 };
 
@@ -839,7 +845,7 @@ __device__ inline double cell_adjoint_species(const ColCtx& c, const ColAdj& a, 
   VEb += hzb * 2 * VE * invr;
   // the species' share of the temperature sweep
   Tb += fa.sweep_adj(c, a, F_T, i, gTb, 0.0);
-  fa.cmax_adj(c, a, i);
+  fa.keep_fc(a, i, false);
   a.own(F_T, i, Tb);
   a.own(F_VE, i, VEb);
   a.own(F_VN, i, VNb);
@@ -888,7 +894,7 @@ __device__ inline void cell_adjoint_rest(const ColCtx& c, const ColAdj& a, int i
   VUb += 2 * invr * divvb;
   Tb += fa.sweep_adj(c, a, F_T, i, gTb, dt * kT);
   VUb += fa.sweep_adj(c, a, F_VU, i, divvb, 0.0);
-  fa.cmax_adj(c, a, i);
+  fa.keep_fc(a, i, true);
   a.gmb[i + 1] += gmb;
   a.own(F_T, i, Tb);
   a.own(F_VE, i, VEb);
@@ -995,6 +1001,18 @@ __device__ inline void cell_gather(const ColCtx& c, const ColAdj& a, int m, int 
     for (int k = 0; k < 4; ++k) v += ok[k] ? u[jj[k]] * mc[k] : 0.0;
     a.x((s < NS) ? F_LNS + s : F_LRHO, m) += (s < NS) ? v : -v;
   }
+  // cMax of cell m: the dissipation coefficients of the faces whose max
+  // took it (cells m and m+1 at their lower faces, cells m-1 and m at their
+  // upper faces), in that order
+  {
+    double cb = 0.0;
+    const double cmm = c.cm(m - (m > -1 ? 1 : 0)), cm0 = c.cm(m), cmp = c.cm(m + (m < nA + 2 ? 1 : 0));
+    if (m + 1 >= 1 && m + 1 <= nA && cm0 >= cmp) cb += a.fb[m];              // cell m+1, lower face
+    if (m >= 1 && m <= nA && !(cmm >= cm0)) cb += a.fb[m - 1];               // cell m, lower face
+    if (m >= 1 && m <= nA && cm0 >= cmp) cb += a.fb[nA + m - 1];             // cell m, upper face
+    if (m - 1 >= 1 && m - 1 <= nA && !(cmm >= cm0)) cb += a.fb[nA + m - 2];  // cell m-1, upper face
+    a.cmb[m + 1] += cb;
+  }
   // the edge shares (interior cells): t = this cell's thread
   if (m >= 1 && m <= nA) {
     const int t = t0 + m - 1;
@@ -1091,6 +1109,7 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       a.obp = col + L.OP;
       a.db = col + A.DB;
       a.gu = col + A.GU;
+      a.fb = col + A.FB;
       a.cmb = col + A.CMB;
       a.gmb = col + A.GMB;
       a.tub = col + A.TUB;
@@ -1376,7 +1395,9 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
       a.x(F_VU, i) += y_vu;
       a.x(F_T, i) += ytemp / tu;
       a.tub[i + 1] += -(ytemp * T4 / tu) / tu;
-      if (heat) atomicAdd(&a.mmb[2], ytemp * dt * hq);
+      // the heating factor's adjoint of each interior cell, summed in cell
+      // order below (GradLogConS's buffer is free until the stage adjoints)
+      if (interior && b.heating && B.heating_scale) a.gu[i - 1] = heat ? ytemp * dt * hq : 0.0;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         a.x(F_W + s, i) += y_w[s];
@@ -1400,6 +1421,12 @@ __global__ void __launch_bounds__(NT, 1) vert_adjoint_kernel(const AParams kp) {
     }
     __syncthreads();  // @phase 5
     boundaries_adjoint(1);  // X4's boundaries: pre-boundary ghosts are Orig's
+    if (tid < nc && !sfrozen[tid] && b.heating && B.heating_scale) {
+      const double* hv = sm + size_t(A.stride) * tid + A.GU;
+      double sum = 0.0;
+      for (int i = 0; i < nA; ++i) sum += hv[i];
+      sm[size_t(A.stride) * tid + A.MMB + 2] += sum;
+    }
     __syncthreads();  // @phase 6
     // combination^T of the final: X4pre = Orig + (K0 + 2K1 + 2K2 + K3) / 6
     if (item) {

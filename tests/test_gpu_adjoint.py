@@ -132,6 +132,19 @@ def test_adjoint_other_altitude_counts(cuda, n_alts):
         assert _rel(g, w) < 1e-9, (n_alts, k, _rel(g, w))
 
 
+def test_adjoint_is_reproducible(cuda):
+    """Every sum of the adjoint kernel has a fixed order (no atomics of
+    floating-point values): two runs give the same bits."""
+    p = abi.default_params()
+    m = synthetic.make_member(40, 50, seed=79, with_heating=True)
+    gen = torch.Generator().manual_seed(8)
+    y = _ybar(m, gen, cuda)
+    a, _ = _gpu_vjp(m, p, 2.0, y)
+    b, _ = _gpu_vjp(m, p, 2.0, y)
+    for k in a:
+        assert torch.equal(a[k], b[k]), k
+
+
 @pytest.mark.parametrize("every", [2, 0])
 def test_rollout_equals_stepwise_composition(cuda, every):
     """Checkpoints every 2 steps, and every step's stages kept (every = 0)."""
