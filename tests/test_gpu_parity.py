@@ -68,6 +68,33 @@ def test_step_matches_oracle(torch_cuda, oracle_lib, variant):
     np.testing.assert_array_equal(st, st_ref)
 
 
+@pytest.mark.parametrize("case", range(12))
+def test_random_parameter_combinations(torch_cuda, oracle_lib, case):
+    """Seeded draws over the switches of the path taken together (solver,
+    friction, ion advection and its form, the MSIS lower boundary, damping,
+    Coriolis, the nighttime ion boundary, producers on the device or given,
+    the limiter's beta, thermal diffusion, a low wind clamp, the heating
+    line) and over nAlts, two steps, against the oracle."""
+    rng = np.random.default_rng(1000 + case)
+    flags = {k: int(rng.integers(0, 2)) for k in ("use_neutral_friction", "use_ion_advection",
+                                                   "use_improved_ion_advection", "use_msis_bcs",
+                                                   "use_damping", "use_coriolis", "use_nighttime_ion_bcs",
+                                                   "compute_coefficients")}
+    solver = abi.SOLVER_AUSM if rng.random() < 0.35 else abi.SOLVER_RUSANOV
+    over = dict(flags, solver=solver, beta_limiter=float(rng.choice([1.0, 1.5, 2.0])),
+                max_vertical_velocity=float(rng.choice([1000.0, 5.0])))
+    if rng.random() < 0.5:
+        over["thermal_diff_coef"] = [0.0, 0.0, 0.0, 0.0, -0.2, -0.38]
+    p = abi.default_params(**over)
+    n_alts = int(rng.choice([20, 50, 64]))
+    m = synthetic.make_member(40, n_alts, seed=2000 + case, with_lbc=bool(flags["use_msis_bcs"]),
+                              with_heating=bool(rng.integers(0, 2)))
+    ref, st_ref = ref_advance(oracle_lib, m, p, 2.0, n_steps=2)
+    out, st = gpu_advance(m, p, 2.0, n_steps=2, config=dict(steps_per_launch=1))
+    assert_state_close(out, ref, STATE)
+    np.testing.assert_array_equal(st, st_ref)
+
+
 @pytest.mark.parametrize("n_steps", [1, 4])
 def test_heating_update(torch_cuda, oracle_lib, n_steps):
     """The add_sources temperature line after each step, resident steps included."""
