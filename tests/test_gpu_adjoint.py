@@ -132,6 +132,32 @@ def test_adjoint_other_altitude_counts(cuda, n_alts):
         assert _rel(g, w) < 1e-9, (n_alts, k, _rel(g, w))
 
 
+@pytest.mark.parametrize("case", range(6))
+def test_adjoint_random_parameter_combinations(cuda, case):
+    """Seeded draws over the switches the adjoint differentiates through
+    (friction, ion advection and its form, the MSIS lower boundary, damping,
+    Coriolis, the nighttime ion boundary, the limiter's beta, the heating
+    line) and over nAlts, against autograd through the transcription."""
+    rng = np.random.default_rng(3000 + case)
+    flags = {k: int(rng.integers(0, 2)) for k in ("use_neutral_friction", "use_ion_advection",
+                                                   "use_improved_ion_advection", "use_msis_bcs",
+                                                   "use_damping", "use_coriolis", "use_nighttime_ion_bcs")}
+    p = abi.default_params(beta_limiter=float(rng.choice([1.0, 2.0])), **flags)
+    n_alts = int(rng.choice([20, 50]))
+    m = synthetic.make_member(16, n_alts, seed=4000 + case, with_lbc=bool(flags["use_msis_bcs"]),
+                              with_heating=bool(rng.integers(0, 2)))
+    gen = torch.Generator().manual_seed(9 + case)
+    y = _ybar(m, gen, cuda)
+    want = _torch_vjp(m, p, 2.0, y, cuda)
+    got, status = _gpu_vjp(m, p, 2.0, y)
+    assert status == (0, 0)
+    for k, w in want.items():
+        g = got[k]
+        if k == "idensity_s":
+            g, w = g[:9], w[:9]
+        assert _rel(g, w) < 1e-9, (flags, k, _rel(g, w))
+
+
 def test_adjoint_is_reproducible(cuda):
     """Every sum of the adjoint kernel has a fixed order (no atomics of
     floating-point values): two runs give the same bits."""
