@@ -213,6 +213,36 @@ def test_ragged_batch(torch_cuda, oracle_lib):
         assert_state_close(dm.to_numpy(), ref, STATE)
 
 
+@pytest.mark.parametrize("case", range(6))
+def test_random_ragged_plans(torch_cuda, oracle_lib, case):
+    """Seeded ragged plans (3 to 5 members of nAlts 8 to 100 and 3 to 40
+    columns) under a random launch configuration of the plan API (a built
+    thread count, columns per CTA, steps per launch, CTAs per SM), three
+    steps, every member against the oracle."""
+    from gitm_b200 import vertical as V
+    rng = np.random.default_rng(5000 + case)
+    solver = abi.SOLVER_AUSM if case % 3 == 2 else abi.SOLVER_RUSANOV
+    p = abi.default_params(solver=solver)
+    n_m = int(rng.integers(3, 6))
+    ms = [synthetic.make_member(int(rng.integers(3, 41)), int(rng.choice([8, 20, 50, 64, 100])),
+                                seed=6000 + 10 * case + i, with_heating=bool(rng.integers(0, 2)))
+          for i in range(n_m)]
+    refs = [ref_advance(oracle_lib, m, p, 2.0, n_steps=3)[0] for m in ms]
+    ctx = V.VerticalContext(p)
+    dms = [V.device_member(m) for m in ms]
+    plan = V.Plan(ctx, dms)
+    threads = [128, 256] if solver == abi.SOLVER_AUSM else [128, 160, 192, 256, 320, 384, 512]
+    cfg = dict(threads=int(rng.choice(threads)), cols_per_cta=int(rng.choice([0, 1, 2])),
+               steps_per_launch=int(rng.choice([1, 2, 3])), ctas_per_sm=int(rng.choice([0, 1, 2])))
+    plan.set_config(**cfg)
+    plan.advance(2.0, 3)
+    plan.check()
+    for dm, ref in zip(dms, refs):
+        assert_state_close(dm.to_numpy(), ref, STATE, rtol=1e-9)
+    plan.close()
+    ctx.close()
+
+
 def test_neg_density_status(torch_cuda, oracle_lib):
     p = abi.default_params()
     m = synthetic.make_member(12, 50, seed=26)
