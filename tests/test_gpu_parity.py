@@ -335,11 +335,15 @@ def test_globe5deg_100_steps_each_against_the_oracle(torch_cuda, oracle_lib):
     print(f"100 steps of 2592 columns: worst per-step normwise rel err {worst:.3e}")
 
 
-def test_modvertical_form(torch_cuda, oracle_lib):
+@pytest.mark.parametrize("variant,n_alts", [("default", 50), ("default", 20), ("no_friction", 64),
+                                            ("log_ions", 50), ("given_coefficients", 30), ("beta1", 100)])
+def test_modvertical_form(torch_cuda, oracle_lib, variant, n_alts):
+    """The advance_vertical_1d_rusanov argument form (ModVertical arrays)
+    against the oracle over parameter variants and nAlts."""
     import torch
     from gitm_b200 import vertical as V
-    p = abi.default_params()
-    m = synthetic.make_member(48, 50, seed=29)
+    p = abi.default_params(**VARIANTS[variant])
+    m = synthetic.make_member(48, n_alts, seed=29 + n_alts)
     d = synthetic.to_modvertical(m, p)
     ref = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
     oracle_lib.advance_1d(ref, p, 2.0)
