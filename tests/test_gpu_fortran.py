@@ -106,7 +106,9 @@ def state_struct(n_alts, n_blk, getptr):
 
 
 @pytest.mark.parametrize("on_device", [0, 1])
-@pytest.mark.parametrize("n_blk,n_alt", [(2, 30), (4, 50)], ids=["2blocks_nalts30", "4blocks_nalts50"])
+@pytest.mark.parametrize("n_blk,n_alt", [(2, 30), (4, 50), (1, 8), (3, 64), (5, 100)],
+                         ids=["2blocks_nalts30", "4blocks_nalts50", "1block_nalts8", "3blocks_nalts64",
+                              "5blocks_nalts100"])
 def test_fortran_layout_matches_oracle(oracle_lib, on_device, n_blk, n_alt):
     import torch
     from gitm_b200 import _lib
