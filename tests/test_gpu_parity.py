@@ -369,6 +369,20 @@ def test_cfl_timestep(torch_cuda, oracle_lib):
     assert V.calc_timestep_vertical(ctx, [dm], cfl=0.75, dt=0.5) == 0.5
 
 
+def test_cfl_timestep_ragged_members(torch_cuda, oracle_lib):
+    """calc_timestep_vertical over members of different nAlts and sizes:
+    the minimum over all their columns (the reference's MPI_Allreduce MIN
+    over blocks), and dt_end when it is smaller."""
+    from gitm_b200 import vertical as V
+    p = abi.default_params()
+    ms = [synthetic.make_member(n, na, seed=90 + i) for i, (n, na) in enumerate([(77, 20), (500, 50), (33, 100)])]
+    want = min(oracle_lib.cfl_dt(m, p, 0.6) for m in ms)
+    ctx = V.VerticalContext(p)
+    dms = [V.device_member(m) for m in ms]
+    assert V.calc_timestep_vertical(ctx, dms, cfl=0.6) == pytest.approx(want, rel=1e-14)
+    assert V.calc_timestep_vertical(ctx, dms, cfl=0.6, dt_end=0.5 * want) == 0.5 * want
+
+
 def test_graph_capture_replays(torch_cuda, oracle_lib):
     import torch
     from gitm_b200 import vertical as V
