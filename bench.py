@@ -148,7 +148,8 @@ class ClockSampler:
                     try:
                         self.samples.append((float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)),
                                              int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)),
-                                             n.nvmlDeviceGetPowerUsage(self.handle) / 1e3))
+                                             n.nvmlDeviceGetPowerUsage(self.handle) / 1e3,
+                                             n.nvmlDeviceGetTemperature(self.handle, n.NVML_TEMPERATURE_GPU)))
                     except Exception:
                         pass
                     self.stop_flag.wait(self.interval)
@@ -169,11 +170,13 @@ class ClockSampler:
         if self.thread is not None:
             self.stop_flag.set()
             self.thread.join(timeout=5)
-            sm = [a for a, _, _ in self.samples]
-            reasons = sorted({name for _, r, _ in self.samples for name, bit in self.REASONS if r & bit})
+            sm = [a for a, _, _, _ in self.samples]
+            reasons = sorted({name for _, r, _, _ in self.samples for name, bit in self.REASONS if r & bit})
             return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "sm_min_mhz": min(sm) if sm else None,
                     "reasons": reasons, "samples": len(sm),
-                    "power_w_max": max((p for _, _, p in self.samples), default=None),
+                    "power_w_max": max((p for _, _, p, _ in self.samples), default=None),
+                    "temp_c_max": max((t for _, _, _, t in self.samples), default=None),
                     "source": f"NVML every {1e3 * self.interval:g} ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
@@ -700,6 +703,8 @@ def run_adjoint(args, fd_directions: int | None = None):
         return g, e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3, float(J.detach())
 
     grads_once(args.adj_steps)  # warm-up at full length (plans, scratch, the saved-state buffers)
+    clocks = ClockSampler(local)  # over every timed part of the leg
+    clocks.start()
     # plain forward of the same rollout: one launch per step, no checkpoints
     torch.cuda.synchronize()
     f0, f1 = ev(), ev()
@@ -769,6 +774,7 @@ def run_adjoint(args, fd_directions: int | None = None):
         t_adj += a2.elapsed_time(a3) / 1e3
     t_save /= n_k
     t_adj /= n_k
+    clk = clocks.stop()
     del sbuf
 
     # finite differences: directions on one column each, eps = 1e-7 relative,
@@ -837,6 +843,7 @@ def run_adjoint(args, fd_directions: int | None = None):
                                                "how": "the two launches of a backward step on fixed buffers, "
                                                       "CUDA events around each, mean of 10"},
                "timing": "median of 3 timed rollouts",
+               "clocks": clk,
                "stages_kept": kept,
                "backward_includes": "segment recompute (the step kernel saving its stage states; the last "
                                     "segment's were kept by the forward) + one adjoint kernel per step "
