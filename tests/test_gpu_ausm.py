@@ -143,3 +143,50 @@ def test_ausm_autotune(torch_cuda):
     cfg = plan.autotune(2.0, 2)
     assert cfg.threads in (128, 256, 384)
     np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
+
+
+def test_unbuilt_shape_is_refused_and_plan_keeps_working(torch_cuda, oracle_lib):
+    """The AUSM 384-thread shape is compiled for nAlts = 50 only: a plan of
+    another nAlts refuses it with an error, keeps its launch shape and still
+    steps like the oracle."""
+    from gitm_b200 import vertical as V
+    p = ausm()
+    m = synthetic.make_member(40, 30, seed=52)
+    ctx = V.VerticalContext(p)
+    dm = V.device_member(m)
+    plan = V.Plan(ctx, [dm])
+    before = plan.config
+    with pytest.raises(V.GitmError, match="not built"):
+        plan.set_config(threads=384)
+    after = plan.config
+    assert (after.threads, after.steps_per_launch) == (before.threads, before.steps_per_launch)
+    np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
+    plan.advance(2.0, 1)
+    plan.check()
+    ref, _ = ref_advance(oracle_lib, m, p, 2.0)
+    assert_state_close(dm.to_numpy(), ref, STATE)
+    plan.close()
+    ctx.close()
+
+
+def test_ausm_autotune_ragged(torch_cuda, oracle_lib):
+    """The autotuner over members of nAlts 50, 75 and 30 picks one of the
+    shapes built for such a plan, leaves the state as it was, and the chosen
+    shape steps like the oracle over two steps."""
+    from gitm_b200 import vertical as V
+    p = ausm()
+    ms = [synthetic.make_member(n, na, seed=53 + i) for i, (n, na) in enumerate([(200, 50), (90, 75), (150, 30)])]
+    ctx = V.VerticalContext(p)
+    dms = [V.device_member(m) for m in ms]
+    plan = V.Plan(ctx, dms)
+    cfg = plan.autotune(2.0, 2)
+    assert cfg.threads in (128, 256)
+    for dm, m in zip(dms, ms):
+        np.testing.assert_array_equal(dm.tensors["ndensity_s"].cpu().numpy(), m.ndensity_s)
+    plan.advance(2.0, 2)
+    plan.check()
+    for dm, m in zip(dms, ms):
+        ref, _ = ref_advance(oracle_lib, m, p, 2.0, n_steps=2)
+        assert_state_close(dm.to_numpy(), ref, STATE, rtol=1e-9)
+    plan.close()
+    ctx.close()
