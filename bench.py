@@ -580,8 +580,11 @@ def e2e_leg(torch, V, ctx, m, n_steps: int, world: int, dev, optional_outputs: b
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    calls = []
     for _ in range(n_steps):
-        V.advance_vertical_all_host(ctx, [pinned], DT, 1)
+        c0 = time.perf_counter()
+        V.advance_vertical_all_host(ctx, [pinned], DT, 1)  # returns with the copies out done
+        calls.append(time.perf_counter() - c0)
     torch.cuda.synchronize()
     ee = time.perf_counter() - t0
     if world > 1:
@@ -590,6 +593,8 @@ def e2e_leg(torch, V, ctx, m, n_steps: int, world: int, dev, optional_outputs: b
         ee = float(t.item())
     return {"value": m.n_cols * n_steps * world / ee, "unit": UNIT,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "call_ms": {"median": 1e3 * statistics.median(calls), "min": 1e3 * min(calls),
+                        "max": 1e3 * max(calls)},
             "how": "gitm_vert_advance_native_host per step: the pinned host arrays advance_vertical "
                    "reads copied in, stepped, the state it writes copied out"
                    + (" with the optional LogNS and NDensity outputs" if optional_outputs else "")
