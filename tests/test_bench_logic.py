@@ -62,3 +62,37 @@ def test_tile_member_repeats_columns_and_keeps_the_grid():
     np.testing.assert_array_equal(t.ndensity_s, m.ndensity_s[..., idx])
     np.testing.assert_array_equal(t.temperature, m.temperature[..., idx])
     np.testing.assert_array_equal(t.altitude, m.altitude)
+
+
+def test_reference_arm_prints_the_contract_line():
+    """bench.py --impl reference on a small globe: one JSON line with the
+    reference arm's keys, its e2e moving no bytes between host and device."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1", "--deg", "10", "--cpu-seconds", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "column-steps/s" and line["value"] > 0
+    assert line["config"]["workload"] == bench.workload_name(10.0, 648, 50, "rusanov")
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": "column-steps/s",
+                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    """Under torchrun only rank 0 of the reference arm works and prints."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1", "--deg", "10", "--cpu-seconds", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=root, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
